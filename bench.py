@@ -1,0 +1,307 @@
+"""Benchmark: exact swap deltas/s of the pairwise sweep at N=18,524.
+
+Workload (the reference-scale pairwise sweep): a synthetic graph pair with
+N=18,524 vertices and 5,000,000 directed G1 edges (power-law out-degree,
+exponent 2.1; weights 1+Geometric(0.35) with a 1e-3 heavy tail capped at
+30,000, so 16-bit storage is exact), G2 = G1 relabelled with 10% of edges
+deleted, 10% added and weights jittered; the initial matching is uniform
+random.  One step = one full sweep: all 171,567,726 pair deltas, best
+partner per vertex, sorted set commit.  The timed region runs on inputs
+already resident in HBM (the profit matrix alone is 1.37 GB, far above the
+126 MB L2).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+
+--impl reference times the reference's own calculate_swap_delta
+(src/graph-alignment-optimized.c:321-408, compiled in place into
+oracle/_ref/librefgao.so) under OpenMP on the host cores, row by row as
+src/alignment-omp.c:601-622 drives it, on a bounded sample of rows.
+Multi-GPU runs are independent replicas (one instance per rank, weak scaling).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "brain-match_b200"))
+
+WORKLOADS = {
+    "n18524_e5m": dict(n=18524, e=5_000_000, wmax=30000, tail_prob=1e-3, seed=20261204),
+    "n1000_e20k": dict(n=1000, e=20_000, wmax=5000, tail_prob=0.0, seed=20261203),
+}
+OWN_KERNELS_PER_SWEEP = 9  # relabel x4, row_work, profit, combine, candidates, commit
+CUB_KERNELS_PER_SWEEP = 2 * 9  # two 64-bit radix sorts (1 histogram + 8 passes each)
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples (200 ms) during the timed region."""
+
+    def __init__(self, dev):
+        self.dev = dev
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev),
+                 "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            try:
+                sm.append(float(f[0]))
+                mx = max(mx, float(f[1]))
+            except (ValueError, IndexError):
+                continue
+            for nm, v in zip(names, f[2:]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return world, rank, local, pg
+
+
+def allreduce_max(pg, x):
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def cpu_reference(g, rows_target_s, seed=5, rows=None):
+    """Times the reference's calculate_swap_delta under OpenMP on a row sample."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    R = oracle.RefGAO()
+    n = g["n"]
+    t0 = time.perf_counter()
+    gm = R.graph(g["src1"], g["dst1"], g["w1"])
+    gf = R.graph(g["src2"], g["dst2"], g["w2"])
+    build_s = time.perf_counter() - t0
+    rng = np.random.default_rng(seed)
+    m = g["map0"]
+    if rows is None:
+        probe = rng.choice(np.arange(1, n + 1), 4, replace=False).astype(np.int32)
+        t = time.perf_counter()
+        R.rows_omp(gm, gf, m, probe, n)
+        dt = max(time.perf_counter() - t, 1e-3)
+        rows = int(min(2048, max(4, 4 * rows_target_s / dt)))
+    sample = rng.choice(np.arange(1, n + 1), rows, replace=False).astype(np.int32)
+    t = time.perf_counter()
+    cnt, checksum, threads = R.rows_omp(gm, gf, m, sample, n)
+    dt = time.perf_counter() - t
+    return dict(value=cnt / dt, deltas=cnt, seconds=dt, rows=rows, threads=threads, build_s=build_s,
+                R=R, gm=gm, gf=gf, checksum=checksum)
+
+
+def run_reference(args, g, world, rank, pg):
+    wl = args.workload
+    if rank != 0:
+        return
+    n = g["n"]
+    per_step = max(1.0, 120.0 / max(1, args.steps + args.warmup))
+    first = cpu_reference(g, per_step)
+    rows = first["rows"]
+    vals = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_reference_step(first, g, rows, seed=100 + i)
+        if i >= args.warmup:
+            vals.append(r)
+    tot_d = sum(v[0] for v in vals)
+    tot_s = sum(v[1] for v in vals)
+    value = tot_d / tot_s
+    line = {
+        "impl": "reference", "metric": "exact swap deltas/s", "value": value, "unit": "deltas/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * tot_s / len(vals), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": wl, "n": n, "e1": int(len(g["src1"])), "e2": int(len(g["src2"])),
+                   "step": f"{rows} full rows of pair deltas (bounded sample of one sweep)"},
+        "cpu_baseline": {"value": value, "unit": "deltas/s", "cores": first["threads"], "kind": "reference",
+                         "sample": f"{rows} seeded rows x {n - 1} partners per step, OpenMP dynamic"},
+        "e2e": {"value": value, "unit": "deltas/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def cpu_reference_step(ctx, g, rows, seed):
+    R, gm, gf = ctx["R"], ctx["gm"], ctx["gf"]
+    n = g["n"]
+    rng = np.random.default_rng(seed)
+    sample = rng.choice(np.arange(1, n + 1), rows, replace=False).astype(np.int32)
+    t = time.perf_counter()
+    cnt, _, _ = R.rows_omp(gm, gf, g["map0"], sample, n)
+    return cnt, time.perf_counter() - t
+
+
+def run_engine(args, g, world, rank, local, pg):
+    import bm
+    import torch
+    torch.cuda.set_device(local)
+    n = g["n"]
+    E = bm.Engine.from_pair(g)
+    info = E.info()
+    E.set_mapping(g["map0"])
+    deltas_per_sweep = n * (n - 1) // 2
+    for _ in range(args.warmup):
+        E.sweep()
+    barrier(pg)
+    torch.cuda.synchronize()
+    stats = []
+    with Clocks(local) as clk:
+        E.timer_mark(0)
+        for _ in range(args.steps):
+            stats.append(E.sweep())
+        E.timer_mark(1)
+        torch.cuda.synchronize()
+    barrier(pg)
+    ms = E.timer_elapsed(0, 1)
+    ms_max = allreduce_max(pg, ms)
+    value = world * args.steps * deltas_per_sweep / (ms_max / 1e3)
+
+    # end to end through the C ABI with host buffers: H2D of the matching,
+    # sweep, D2H of the matching and the score
+    host_map = E.get_mapping()
+    e2e_steps = max(3, args.steps)
+    barrier(pg)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        E.set_mapping(host_map)
+        st = E.sweep()
+        host_map = E.get_mapping()
+        _ = st["score_after"]
+    t1 = time.perf_counter()
+    e2e_s = allreduce_max(pg, t1 - t0)
+    e2e_value = world * e2e_steps * deltas_per_sweep / e2e_s
+    h2d = 2 * (n + 1) * 4
+    d2h = (n + 1) * 4 + 8 + 96
+
+    # roofline of the dominant kernel (profit rows), timed live with events
+    prof_ms = statistics.mean(s["ms_profit"] for s in stats)
+    alg_bytes = 2 * n * n * (info["entry_bits"] // 8)   # W1 and P2 once, per sweep
+    peak, peak_kind = peaks()
+    achieved = alg_bytes / (prof_ms / 1e3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "k_profit_traffic.json")
+    if os.path.exists(tp):
+        try:
+            traffic = json.load(open(tp)).get("bytes_per_launch_full_size")
+        except (OSError, ValueError):
+            traffic = None
+    terms = statistics.mean(s["min_terms"] for s in stats)
+
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu:
+            try:
+                c = cpu_reference(g, args.cpu_seconds)
+                cpu = {"value": c["value"], "unit": "deltas/s", "cores": c["threads"], "kind": "reference",
+                       "sample": f"{c['rows']} seeded rows x {n - 1} partners ({c['deltas']} deltas, "
+                                 f"{c['seconds']:.1f} s), reference calculate_swap_delta under OpenMP"}
+            except OSError as e:
+                cpu = {"value": None, "unit": "deltas/s", "cores": 0, "kind": "reference", "sample": str(e)}
+        line = {
+            "metric": "exact swap deltas/s", "value": value, "unit": "deltas/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic",
+            "config": {"workload": args.workload, "n": n, "e1": int(info["e1"]), "e2": int(info["e2"]),
+                       "entry_bits": info["entry_bits"], "step": "full pairwise sweep + set commit",
+                       "deltas_per_step": deltas_per_sweep, "l2": "inputs larger than L2",
+                       "parallelism": f"replicas{world}"},
+            "e2e": {"value": e2e_value, "unit": "deltas/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "steps": e2e_steps},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "k_profit", "kernel_ms": prof_ms, "alg_bytes": alg_bytes,
+                         "min_terms": terms},
+            "cpu_baseline": cpu,
+            "gpu_launches": args.steps * (OWN_KERNELS_PER_SWEEP + CUB_KERNELS_PER_SWEEP),
+            "clocks": clk.summary(),
+            "sweeps": [{k: s[k] for k in ("score_before", "score_after", "committed", "verified", "candidates",
+                                         "ms_prep", "ms_profit", "ms_combine", "ms_commit", "ms_total",
+                                         "min_terms")} for s in stats],
+        }
+        print(json.dumps(line), flush=True)
+    E.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--workload", default="n18524_e5m", choices=sorted(WORKLOADS))
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    world, rank, local, pg = dist_setup()
+    import bm
+    p = dict(WORKLOADS[args.workload])
+    p["seed"] += rank  # independent replica per rank
+    g = bm.generate(bm.gen_params(**p))
+    if args.impl == "reference":
+        run_reference(args, g, world, rank, pg)
+    else:
+        run_engine(args, g, world, rank, local, pg)
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

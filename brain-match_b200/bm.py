@@ -1,0 +1,272 @@
+"""ctypes binding of the engine's C ABI (include/bm.h) for tests and bench.
+
+The engine itself is libbm.so (CUDA kernels for sm_100a + host C).  This module
+only marshals numpy arrays across the C boundary; there is no Python or CPU
+fallback for any compute call -- if the library is missing, loading fails.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libbm.so")
+
+BM_OK, BM_E_INPUT, BM_E_CUDA, BM_E_OVERFLOW, BM_E_TIMEOUT, BM_E_NOMEM, BM_E_STATE, BM_E_IO = (
+    0, -1, -2, -3, -4, -5, -6, -7)
+BM_FLAG_FORCE_I32 = 1
+
+
+class GenParams(C.Structure):
+    _fields_ = [("n", C.c_int32), ("wmax", C.c_int32), ("e", C.c_int64), ("seed", C.c_uint64),
+                ("alpha", C.c_double), ("geom_p", C.c_double), ("tail_prob", C.c_double),
+                ("tail_alpha", C.c_double), ("tail_scale", C.c_double), ("del_frac", C.c_double),
+                ("add_frac", C.c_double), ("jitter", C.c_int32), ("reserved", C.c_int32)]
+
+
+class Info(C.Structure):
+    _fields_ = [("n", C.c_int32), ("entry_bits", C.c_int32), ("e1", C.c_int64), ("e2", C.c_int64),
+                ("g1_self_loops", C.c_int64), ("device_bytes", C.c_int64), ("device", C.c_int32),
+                ("num_sms", C.c_int32)]
+
+
+class SweepOpts(C.Structure):
+    _fields_ = [("max_candidates", C.c_int32), ("max_verify", C.c_int32), ("reserved", C.c_int32 * 6)]
+
+
+class SweepStats(C.Structure):
+    _fields_ = [("score_before", C.c_int64), ("score_after", C.c_int64), ("deltas_evaluated", C.c_int64),
+                ("candidates", C.c_int32), ("scanned", C.c_int32), ("verified", C.c_int32),
+                ("committed", C.c_int32), ("best_delta", C.c_int32), ("reserved", C.c_int32),
+                ("ms_profit", C.c_float), ("ms_combine", C.c_float), ("ms_commit", C.c_float),
+                ("ms_total", C.c_float), ("ms_prep", C.c_float), ("pad", C.c_int32), ("min_terms", C.c_int64)]
+
+
+class TripleOpts(C.Structure):
+    _fields_ = [("partners", C.c_int32), ("max_candidates", C.c_int32), ("max_verify", C.c_int32),
+                ("reserved0", C.c_int32), ("seed", C.c_uint64), ("reserved", C.c_int32 * 4)]
+
+
+class TripleStats(C.Structure):
+    _fields_ = [("score_before", C.c_int64), ("score_after", C.c_int64), ("triples", C.c_int64),
+                ("rotations", C.c_int64), ("candidates", C.c_int32), ("scanned", C.c_int32),
+                ("verified", C.c_int32), ("committed", C.c_int32), ("best_delta", C.c_int32),
+                ("reserved", C.c_int32), ("ms_sample", C.c_float), ("ms_eval", C.c_float),
+                ("ms_commit", C.c_float), ("ms_total", C.c_float)]
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+_lib = None
+
+
+def lib():
+    """Loads libbm.so (raises OSError when it has not been built)."""
+    global _lib
+    if _lib is None:
+        L = C.CDLL(LIB_PATH)
+        vp, i32, i64, u32 = C.c_void_p, C.c_int32, C.c_int64, C.c_uint32
+        L.bm_status_string.restype = C.c_char_p
+        L.bm_status_string.argtypes = [i32]
+        L.bm_last_error.restype = C.c_char_p
+        L.bm_last_error.argtypes = [vp]
+        L.bm_create.argtypes = [C.POINTER(vp), i32, i64, vp, vp, vp, i64, vp, vp, vp, u32]
+        L.bm_destroy.argtypes = [vp]
+        L.bm_destroy.restype = None
+        L.bm_get_info.argtypes = [vp, C.POINTER(Info)]
+        for f in ("bm_set_mapping", "bm_get_mapping", "bm_all_deltas"):
+            getattr(L, f).argtypes = [vp, vp]
+        L.bm_score.argtypes = [vp, C.POINTER(i64)]
+        L.bm_pair_deltas.argtypes = [vp, i64, vp, vp, vp]
+        L.bm_profit_row.argtypes = [vp, i32, vp]
+        L.bm_sweep.argtypes = [vp, C.POINTER(SweepOpts), C.POINTER(SweepStats)]
+        L.bm_hillclimb.argtypes = [vp, i32, C.POINTER(SweepOpts), vp, C.POINTER(i32)]
+        L.bm_first_improvement.argtypes = [vp, i32, C.POINTER(i64), C.POINTER(i32)]
+        L.bm_triple_deltas.argtypes = [vp, i64, vp, vp, vp, vp]
+        L.bm_triple_round.argtypes = [vp, C.POINTER(TripleOpts), C.POINTER(TripleStats)]
+        L.bm_timer_mark.argtypes = [vp, i32]
+        L.bm_timer_elapsed.argtypes = [vp, i32, i32, C.POINTER(C.c_float)]
+        L.bm_free.argtypes = [vp]
+        L.bm_free.restype = None
+        L.bm_read_graph_csv.argtypes = [C.c_char_p, C.POINTER(i64), C.POINTER(vp), C.POINTER(vp),
+                                        C.POINTER(vp), C.POINTER(i32)]
+        L.bm_read_mapping_csv.argtypes = [C.c_char_p, i32, vp, C.POINTER(i32)]
+        L.bm_write_mapping_csv.argtypes = [C.c_char_p, i32, vp]
+        L.bm_write_mapping_csv_numeric.argtypes = [C.c_char_p, i32, vp]
+        L.bm_gen_defaults.argtypes = [C.POINTER(GenParams)]
+        L.bm_gen_defaults.restype = None
+        L.bm_generate.argtypes = [C.POINTER(GenParams), vp, vp, vp, C.POINTER(i64), vp, vp, vp, vp, vp]
+        _lib = L
+    return _lib
+
+
+class BMError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{lib().bm_status_string(status).decode()} ({status}): {msg}")
+        self.status = status
+
+
+def _check(st, ctx=None):
+    if st != BM_OK:
+        raise BMError(st, (lib().bm_last_error(ctx) or b"").decode())
+
+
+# ---- generator -------------------------------------------------------------
+def gen_params(n=1000, e=20000, seed=20261203, wmax=5000, tail_prob=0.0, **kw):
+    p = GenParams()
+    lib().bm_gen_defaults(C.byref(p))
+    p.n, p.e, p.seed, p.wmax, p.tail_prob = n, e, seed, wmax, tail_prob
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def generate(params):
+    """Runs bm_generate; returns dict of int32 numpy arrays (1-based ids)."""
+    e = params.e
+    cap = e + int(np.ceil(params.add_frac * e)) + 1
+    s1, d1, w1 = (np.zeros(e, np.int32) for _ in range(3))
+    s2, d2, w2 = (np.zeros(cap, np.int32) for _ in range(3))
+    pi = np.zeros(params.n + 1, np.int32)
+    m0 = np.zeros(params.n + 1, np.int32)
+    e2 = C.c_int64()
+    _check(lib().bm_generate(C.byref(params), _p(s1), _p(d1), _p(w1), C.byref(e2), _p(s2), _p(d2),
+                             _p(w2), _p(pi), _p(m0)))
+    k = e2.value
+    return dict(n=params.n, src1=s1, dst1=d1, w1=w1, src2=s2[:k].copy(), dst2=d2[:k].copy(),
+                w2=w2[:k].copy(), pi=pi, map0=m0)
+
+
+# ---- engine ----------------------------------------------------------------
+class Engine:
+    """One engine context on the current CUDA device."""
+
+    def __init__(self, n, src1, dst1, w1, src2, dst2, w2, flags=0):
+        arrs = [np.ascontiguousarray(x, dtype=np.int32) for x in (src1, dst1, w1, src2, dst2, w2)]
+        self._keep = arrs
+        h = C.c_void_p()
+        st = lib().bm_create(C.byref(h), int(n), len(arrs[0]), _p(arrs[0]), _p(arrs[1]), _p(arrs[2]),
+                             len(arrs[3]), _p(arrs[3]), _p(arrs[4]), _p(arrs[5]), flags)
+        _check(st, None)
+        self.h = h
+        self.n = int(n)
+
+    @classmethod
+    def from_pair(cls, g, flags=0):
+        return cls(g["n"], g["src1"], g["dst1"], g["w1"], g["src2"], g["dst2"], g["w2"], flags)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().bm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def info(self):
+        i = Info()
+        _check(lib().bm_get_info(self.h, C.byref(i)), self.h)
+        return {k: getattr(i, k) for k, _ in Info._fields_}
+
+    def set_mapping(self, m):
+        m = np.ascontiguousarray(m, dtype=np.int32)
+        assert m.shape == (self.n + 1,)
+        _check(lib().bm_set_mapping(self.h, _p(m)), self.h)
+
+    def get_mapping(self):
+        m = np.zeros(self.n + 1, np.int32)
+        _check(lib().bm_get_mapping(self.h, _p(m)), self.h)
+        return m
+
+    def score(self):
+        s = C.c_int64()
+        _check(lib().bm_score(self.h, C.byref(s)), self.h)
+        return s.value
+
+    def pair_deltas(self, m1, m2):
+        m1 = np.ascontiguousarray(m1, np.int32)
+        m2 = np.ascontiguousarray(m2, np.int32)
+        out = np.zeros(len(m1), np.int32)
+        _check(lib().bm_pair_deltas(self.h, len(m1), _p(m1), _p(m2), _p(out)), self.h)
+        return out
+
+    def all_deltas(self):
+        out = np.zeros(self.n * (self.n - 1) // 2, np.int32)
+        _check(lib().bm_all_deltas(self.h, _p(out)), self.h)
+        return out
+
+    def profit_row(self, a):
+        out = np.zeros(self.n, np.int32)
+        _check(lib().bm_profit_row(self.h, int(a), _p(out)), self.h)
+        return out
+
+    def sweep(self, max_candidates=0, max_verify=-1):
+        o = SweepOpts(max_candidates, max_verify)
+        s = SweepStats()
+        _check(lib().bm_sweep(self.h, C.byref(o), C.byref(s)), self.h)
+        return {k: getattr(s, k) for k, _ in SweepStats._fields_ if k not in ("reserved", "pad")}
+
+    def timer_mark(self, slot):
+        _check(lib().bm_timer_mark(self.h, slot), self.h)
+
+    def timer_elapsed(self, a, b):
+        ms = C.c_float()
+        _check(lib().bm_timer_elapsed(self.h, a, b, C.byref(ms)), self.h)
+        return ms.value
+
+    def first_improvement(self, max_passes):
+        c, p = C.c_int64(), C.c_int32()
+        _check(lib().bm_first_improvement(self.h, int(max_passes), C.byref(c), C.byref(p)), self.h)
+        return c.value, p.value
+
+    def triple_deltas(self, a, b, c):
+        a, b, c = (np.ascontiguousarray(x, np.int32) for x in (a, b, c))
+        out = np.zeros(2 * len(a), np.int32)
+        _check(lib().bm_triple_deltas(self.h, len(a), _p(a), _p(b), _p(c), _p(out)), self.h)
+        return out.reshape(-1, 2)
+
+    def triple_round(self, partners=256, seed=0, max_candidates=0, max_verify=-1):
+        o = TripleOpts()
+        o.partners, o.max_candidates, o.max_verify, o.seed = partners, max_candidates, max_verify, seed
+        s = TripleStats()
+        _check(lib().bm_triple_round(self.h, C.byref(o), C.byref(s)), self.h)
+        return {k: getattr(s, k) for k, _ in TripleStats._fields_ if k != "reserved"}
+
+
+def read_graph_csv(path):
+    e, s, d, w, mx = C.c_int64(), C.c_void_p(), C.c_void_p(), C.c_void_p(), C.c_int32()
+    _check(lib().bm_read_graph_csv(path.encode(), C.byref(e), C.byref(s), C.byref(d), C.byref(w),
+                                   C.byref(mx)))
+    out = []
+    for ptr in (s, d, w):
+        if e.value:
+            arr = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_int32)), shape=(e.value,)).copy()
+        else:
+            arr = np.zeros(0, np.int32)
+        lib().bm_free(ptr)
+        out.append(arr)
+    return out[0], out[1], out[2], mx.value
+
+
+def read_mapping_csv(path, n):
+    m = np.zeros(n + 1, np.int32)
+    cnt = C.c_int32()
+    _check(lib().bm_read_mapping_csv(path.encode(), n, _p(m), C.byref(cnt)))
+    return m, cnt.value
+
+
+def write_mapping_csv(path, m, numeric=False):
+    m = np.ascontiguousarray(m, np.int32)
+    f = lib().bm_write_mapping_csv_numeric if numeric else lib().bm_write_mapping_csv
+    _check(f(path.encode(), len(m) - 1, _p(m)))

@@ -1,0 +1,783 @@
+// bm_engine.cu -- context, preprocessing and the C ABI of the swap-delta engine.
+//
+// Boundary: include/bm.h.  Every entry point returns a bm_status and records
+// a message retrievable with bm_last_error; nothing here calls exit().
+// All device work of a context runs on one non-blocking stream.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <cstdarg>
+#include <vector>
+#include <algorithm>
+#include <utility>
+#include <cuda_runtime.h>
+#include <cub/device/device_radix_sort.cuh>
+#include "bm.h"
+#include "bm_kernels.cuh"
+#include "bm_triples.cuh"
+
+using namespace bm;
+
+struct bm_ctx {
+    int n = 0;
+    bool w16 = true;
+    int dev = 0, num_sms = 0;
+    long long e1 = 0, e2 = 0, nself = 0;
+    cudaStream_t st = nullptr;
+    char err[512] = {0};
+    bool mapped = false;
+    long long score = 0;  // score of the current matching (kept exact across commits)
+    // device buffers
+    int *off1o = nullptr, *off1i = nullptr, *off2o = nullptr, *off2i = nullptr, *offs = nullptr, *selfw = nullptr;
+    void *ent1o = nullptr, *ent1i = nullptr, *ent2o = nullptr, *ent2i = nullptr;
+    void *ent1oP = nullptr, *ent1iP = nullptr, *ent2oP = nullptr, *ent2iP = nullptr;
+    void* W2 = nullptr;
+    int *p = nullptr, *pinv = nullptr;
+    int* S = nullptr;
+    unsigned long long* rowbest = nullptr;
+    unsigned long long *ckeys = nullptr, *ckeys_sorted = nullptr;
+    unsigned long long *wkeys = nullptr, *wkeys_sorted = nullptr;
+    int *wvals = nullptr, *order = nullptr;
+    void* cub_tmp = nullptr;
+    size_t cub_bytes = 0;
+    int* small = nullptr;          // [0]=row counter [1]=ncand [2]=best delta
+    unsigned long long* score_acc = nullptr;
+    CommitStats* cstats = nullptr;
+    int* scratch_pairs = nullptr;  // pair/triple inputs and outputs (ints)
+    long long scratch_cap = 0;
+    unsigned* adj = nullptr;       // G1 adjacency bitmap (3-cycles)
+    int adj_words = 0;
+    int* rowd = nullptr;           // reference-order row deltas
+    int* first = nullptr;          // [0] = first improving partner, [1] = copy for the host
+    long long* fi_acc = nullptr;   // [0] = delta sum, [1] = commits
+    unsigned long long* tcount = nullptr;
+    long long dev_bytes = 0;
+    cudaEvent_t ev[6] = {};
+    cudaEvent_t uev[8] = {};       // bm_timer_* slots
+    unsigned long long* work_sum = nullptr;
+};
+
+static thread_local char g_create_err[512];
+
+static void set_err(bm_ctx* c, const char* fmt, ...) {
+    char* dst = c ? c->err : g_create_err;
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(dst, 512, fmt, ap);
+    va_end(ap);
+}
+
+#define CK(call)                                                                   \
+    do {                                                                           \
+        cudaError_t e_ = (call);                                                   \
+        if (e_ != cudaSuccess) {                                                   \
+            set_err(ctx, "%s:%d: %s: %s", __FILE__, __LINE__, #call,               \
+                    cudaGetErrorString(e_));                                       \
+            return BM_E_CUDA;                                                      \
+        }                                                                          \
+    } while (0)
+
+template <typename T>
+static cudaError_t dalloc(bm_ctx* ctx, T** ptr, size_t bytes) {
+    cudaError_t e = cudaMalloc((void**)ptr, bytes ? bytes : 16);
+    if (e == cudaSuccess) ctx->dev_bytes += (long long)bytes;
+    return e;
+}
+
+extern "C" const char* bm_last_error(const bm_ctx* ctx) { return ctx ? ctx->err : g_create_err; }
+
+// ---------------------------------------------------------------------------
+// Host preprocessing: CSR/CSC build with the reference's graph semantics.
+namespace {
+
+struct HostCSR {
+    std::vector<int> off;        // n+2 (off[n+1] = off[n]: empty NONE row)
+    std::vector<int> id, w;      // entries
+};
+
+// Builds a CSR keyed by `key` (src for out-lists, dst for in-lists); entries
+// within a row are sorted by the other endpoint, ties kept in input order.
+static void build_csr(int n, const std::vector<int>& key, const std::vector<int>& other,
+                      const std::vector<int>& w, HostCSR& out) {
+    const size_t m = key.size();
+    out.off.assign((size_t)n + 2, 0);
+    for (size_t i = 0; i < m; i++) out.off[key[i] + 1]++;
+    for (int v = 0; v < n; v++) out.off[v + 1] += out.off[v];
+    out.off[n + 1] = out.off[n];
+    std::vector<int> pos(out.off.begin(), out.off.begin() + n);
+    std::vector<int> idx(m);
+    for (size_t i = 0; i < m; i++) idx[pos[key[i]]++] = (int)i;
+    for (int v = 0; v < n; v++) {
+        auto b = idx.begin() + out.off[v], e = idx.begin() + out.off[v + 1];
+        std::stable_sort(b, e, [&](int x, int y) { return other[x] < other[y]; });
+    }
+    out.id.resize(m);
+    out.w.resize(m);
+    for (size_t i = 0; i < m; i++) { out.id[i] = other[idx[i]]; out.w[i] = w[idx[i]]; }
+}
+
+}  // namespace
+
+template <bool W16>
+static DevView<W16> view(bm_ctx* c) {
+    DevView<W16> g;
+    typedef typename Ent<W16>::T E;
+    typedef typename Dense<W16>::T D;
+    g.n = c->n;
+    g.off1o = c->off1o; g.ent1o = (const E*)c->ent1o;
+    g.off1i = c->off1i; g.ent1i = (const E*)c->ent1i;
+    g.off2o = c->off2o; g.ent2o = (const E*)c->ent2o;
+    g.off2i = c->off2i; g.ent2i = (const E*)c->ent2i;
+    g.offs = c->offs; g.selfw = c->selfw;
+    g.ent1oP = (E*)c->ent1oP; g.ent1iP = (E*)c->ent1iP;
+    g.ent2oP = (E*)c->ent2oP; g.ent2iP = (E*)c->ent2iP;
+    g.W2 = (const D*)c->W2;
+    g.p = c->p; g.pinv = c->pinv;
+    g.S = c->S;
+    return g;
+}
+
+template <bool W16>
+static bm_status upload_lists(bm_ctx* ctx, const HostCSR& g1o, const HostCSR& g1i,
+                              const HostCSR& g2o, const HostCSR& g2i, int clamp1, int clamp2) {
+    typedef Ent<W16> EN;
+    typedef typename EN::T E;
+    auto pack = [&](const HostCSR& h, int clampw, void** dst, void** dstP) -> bm_status {
+        std::vector<E> v(h.id.size());
+        for (size_t i = 0; i < v.size(); i++) v[i] = EN::make(h.id[i], std::min(h.w[i], clampw));
+        CK(dalloc(ctx, (E**)dst, v.size() * sizeof(E)));
+        CK(dalloc(ctx, (E**)dstP, v.size() * sizeof(E)));
+        if (!v.empty()) CK(cudaMemcpy(*dst, v.data(), v.size() * sizeof(E), cudaMemcpyHostToDevice));
+        return BM_OK;
+    };
+    bm_status s;
+    if ((s = pack(g1o, clamp1, &ctx->ent1o, &ctx->ent1oP)) != BM_OK) return s;
+    if ((s = pack(g1i, clamp1, &ctx->ent1i, &ctx->ent1iP)) != BM_OK) return s;
+    if ((s = pack(g2o, clamp2, &ctx->ent2o, &ctx->ent2oP)) != BM_OK) return s;
+    if ((s = pack(g2i, clamp2, &ctx->ent2i, &ctx->ent2iP)) != BM_OK) return s;
+    return BM_OK;
+}
+
+template <bool W16>
+static bm_status upload_dense(bm_ctx* ctx, const HostCSR& g2o, int clamp2) {
+    typedef typename Dense<W16>::T D;
+    const size_t n1 = (size_t)ctx->n + 1;
+    CK(dalloc(ctx, (D**)&ctx->W2, n1 * n1 * sizeof(D)));
+    CK(cudaMemset(ctx->W2, 0, n1 * n1 * sizeof(D)));
+    // fill row by row through a pinned staging row
+    std::vector<D> row(n1);
+    const int n = ctx->n;
+    const size_t chunk_rows = 256;
+    std::vector<D> buf(chunk_rows * n1);
+    for (int f0 = 0; f0 < n; f0 += (int)chunk_rows) {
+        const int f1 = std::min(n, f0 + (int)chunk_rows);
+        std::fill(buf.begin(), buf.end(), (D)0);
+        for (int f = f0; f < f1; f++)
+            for (int i = g2o.off[f]; i < g2o.off[f + 1]; i++)
+                buf[(size_t)(f - f0) * n1 + g2o.id[i]] = (D)std::min(g2o.w[i], clamp2);
+        CK(cudaMemcpy((D*)ctx->W2 + (size_t)f0 * n1, buf.data(), (size_t)(f1 - f0) * n1 * sizeof(D),
+                      cudaMemcpyHostToDevice));
+    }
+    return BM_OK;
+}
+
+static void free_ctx(bm_ctx* c) {
+    if (!c) return;
+    void* bufs[] = {c->off1o, c->off1i, c->off2o, c->off2i, c->offs, c->selfw, c->ent1o, c->ent1i,
+                    c->ent2o, c->ent2i, c->ent1oP, c->ent1iP, c->ent2oP, c->ent2iP, c->W2, c->p,
+                    c->pinv, c->S, c->rowbest, c->ckeys, c->ckeys_sorted, c->wkeys, c->wkeys_sorted,
+                    c->wvals, c->order, c->cub_tmp, c->small, c->score_acc, c->cstats, c->scratch_pairs,
+                    c->adj, c->rowd, c->first, c->fi_acc, c->tcount};
+    for (void* b : bufs) if (b) cudaFree(b);
+    for (auto& e : c->ev) if (e) cudaEventDestroy(e);
+    for (auto& e : c->uev) if (e) cudaEventDestroy(e);
+    if (c->work_sum) cudaFree(c->work_sum);
+    if (c->st) cudaStreamDestroy(c->st);
+    delete c;
+}
+
+extern "C" void bm_destroy(bm_ctx* ctx) { free_ctx(ctx); }
+
+extern "C" bm_status bm_create(bm_ctx** out, int32_t n, int64_t e1, const int32_t* src1,
+                               const int32_t* dst1, const int32_t* w1, int64_t e2,
+                               const int32_t* src2, const int32_t* dst2, const int32_t* w2,
+                               uint32_t flags) {
+    if (!out) { set_err(nullptr, "bm_create: out is NULL"); return BM_E_INPUT; }
+    *out = nullptr;
+    if (n < 2 || n > 65535) { set_err(nullptr, "bm_create: n=%d outside 2..65535", n); return BM_E_INPUT; }
+    if (e1 < 0 || e2 < 0 || e1 > 0x7fffffff || e2 > 0x7fffffff ||
+        (e1 && (!src1 || !dst1 || !w1)) || (e2 && (!src2 || !dst2 || !w2))) {
+        set_err(nullptr, "bm_create: bad edge arrays");
+        return BM_E_INPUT;
+    }
+    // ---- validate and split G1 (self-loops apart, zero weights dropped) ----
+    std::vector<int> s1, d1, ww1, selfv, selfwt;
+    s1.reserve(e1); d1.reserve(e1); ww1.reserve(e1);
+    long long maxw1 = 0;
+    for (int64_t i = 0; i < e1; i++) {
+        const int a = src1[i], b = dst1[i], w = w1[i];
+        if (a < 1 || a > n || b < 1 || b > n) { set_err(nullptr, "bm_create: G1 edge %lld has id outside 1..%d", (long long)i, n); return BM_E_INPUT; }
+        if (w < 0) { set_err(nullptr, "bm_create: G1 edge %lld has negative weight %d", (long long)i, w); return BM_E_INPUT; }
+        if (w == 0) continue;
+        maxw1 = std::max<long long>(maxw1, w);
+        if (a == b) { selfv.push_back(a - 1); selfwt.push_back(w); continue; }
+        s1.push_back(a - 1); d1.push_back(b - 1); ww1.push_back(w);
+    }
+    // ---- G2: last weight per (src,dst) wins, as the dense reference matrix does ----
+    std::vector<std::pair<long long, int>> keys2;   // ((src,dst) pair, input index)
+    keys2.reserve(e2);
+    for (int64_t i = 0; i < e2; i++) {
+        const int a = src2[i], b = dst2[i], w = w2[i];
+        if (a < 1 || a > n || b < 1 || b > n) { set_err(nullptr, "bm_create: G2 edge %lld has id outside 1..%d", (long long)i, n); return BM_E_INPUT; }
+        if (w < 0) { set_err(nullptr, "bm_create: G2 edge %lld has negative weight %d", (long long)i, w); return BM_E_INPUT; }
+        keys2.emplace_back((long long)(a - 1) * n + (b - 1), (int)i);
+    }
+    std::sort(keys2.begin(), keys2.end());
+    std::vector<int> s2, d2, ww2;
+    long long maxw2 = 0;
+    for (size_t k = 0; k < keys2.size(); k++) {
+        const long long pair = keys2[k].first;
+        if (k + 1 < keys2.size() && keys2[k + 1].first == pair) continue;  // a later copy wins
+        const int i = keys2[k].second;
+        if (w2[i] == 0) continue;
+        s2.push_back((int)(pair / n)); d2.push_back((int)(pair % n)); ww2.push_back(w2[i]);
+        maxw2 = std::max<long long>(maxw2, w2[i]);
+    }
+    // ---- storage mode: 16-bit when one side's weights fit (min(w1,w2) is unchanged
+    //      by clamping the other side at 65535) ----
+    const bool w16 = !(flags & BM_FLAG_FORCE_I32) && std::min(maxw1, maxw2) <= 65535;
+    const int clamp1 = (w16 && maxw1 > 65535) ? 65535 : 0x7fffffff;
+    const int clamp2 = (w16 && maxw2 > 65535) ? 65535 : 0x7fffffff;
+    // ---- overflow guard: every delta is bounded by 8 x the heaviest vertex load ----
+    {
+        std::vector<long long> load(n, 0);
+        for (size_t i = 0; i < s1.size(); i++) { load[s1[i]] += std::min(ww1[i], clamp1); load[d1[i]] += std::min(ww1[i], clamp1); }
+        for (size_t i = 0; i < selfv.size(); i++) load[selfv[i]] += 2LL * std::min(selfwt[i], clamp1);
+        long long mx = 0;
+        for (int v = 0; v < n; v++) mx = std::max(mx, load[v]);
+        if (mx > 0x7fffffffLL / 8) {
+            set_err(nullptr, "bm_create: vertex weight load %lld could overflow int32 deltas", mx);
+            return BM_E_OVERFLOW;
+        }
+    }
+    HostCSR g1o, g1i, g2o, g2i, gs;
+    build_csr(n, s1, d1, ww1, g1o);
+    build_csr(n, d1, s1, ww1, g1i);
+    build_csr(n, s2, d2, ww2, g2o);
+    build_csr(n, d2, s2, ww2, g2i);
+    {
+        std::vector<int> zero(selfv.size(), 0);
+        build_csr(n, selfv, zero, selfwt, gs);
+        for (auto& x : gs.w) x = std::min(x, clamp1);
+    }
+
+    bm_ctx* ctx = new (std::nothrow) bm_ctx();
+    if (!ctx) { set_err(nullptr, "bm_create: out of host memory"); return BM_E_NOMEM; }
+    ctx->n = n;
+    ctx->w16 = w16;
+    ctx->e1 = (long long)s1.size();
+    ctx->e2 = (long long)s2.size();
+    ctx->nself = (long long)selfv.size();
+    auto fail = [&](bm_status s) {
+        snprintf(g_create_err, sizeof g_create_err, "%s", ctx->err);
+        free_ctx(ctx);
+        return s;
+    };
+    {
+        cudaError_t e = cudaGetDevice(&ctx->dev);
+        if (e != cudaSuccess) { set_err(ctx, "bm_create: no CUDA device: %s", cudaGetErrorString(e)); return fail(BM_E_CUDA); }
+        cudaDeviceProp prop;
+        e = cudaGetDeviceProperties(&prop, ctx->dev);
+        if (e != cudaSuccess) { set_err(ctx, "bm_create: %s", cudaGetErrorString(e)); return fail(BM_E_CUDA); }
+        ctx->num_sms = prop.multiProcessorCount;
+    }
+    auto body = [&]() -> bm_status {
+        CK(cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking));
+        for (auto& e : ctx->ev) CK(cudaEventCreate(&e));
+        for (auto& e : ctx->uev) CK(cudaEventCreate(&e));
+        CK(dalloc(ctx, &ctx->work_sum, sizeof(unsigned long long)));
+        auto up_off = [&](const HostCSR& h, int** d) -> bm_status {
+            CK(dalloc(ctx, d, h.off.size() * sizeof(int)));
+            CK(cudaMemcpy(*d, h.off.data(), h.off.size() * sizeof(int), cudaMemcpyHostToDevice));
+            return BM_OK;
+        };
+        bm_status s;
+        if ((s = up_off(g1o, &ctx->off1o)) || (s = up_off(g1i, &ctx->off1i)) ||
+            (s = up_off(g2o, &ctx->off2o)) || (s = up_off(g2i, &ctx->off2i)) || (s = up_off(gs, &ctx->offs)))
+            return s;
+        CK(dalloc(ctx, &ctx->selfw, gs.w.size() * sizeof(int)));
+        if (!gs.w.empty()) CK(cudaMemcpy(ctx->selfw, gs.w.data(), gs.w.size() * sizeof(int), cudaMemcpyHostToDevice));
+        s = w16 ? upload_lists<true>(ctx, g1o, g1i, g2o, g2i, clamp1, clamp2)
+                : upload_lists<false>(ctx, g1o, g1i, g2o, g2i, clamp1, clamp2);
+        if (s) return s;
+        s = w16 ? upload_dense<true>(ctx, g2o, clamp2) : upload_dense<false>(ctx, g2o, clamp2);
+        if (s) return s;
+        CK(dalloc(ctx, &ctx->p, (n + 1) * sizeof(int)));
+        CK(dalloc(ctx, &ctx->pinv, (n + 1) * sizeof(int)));
+        CK(dalloc(ctx, &ctx->rowbest, n * sizeof(unsigned long long)));
+        CK(dalloc(ctx, &ctx->ckeys, n * sizeof(unsigned long long)));
+        CK(dalloc(ctx, &ctx->ckeys_sorted, n * sizeof(unsigned long long)));
+        CK(dalloc(ctx, &ctx->wkeys, n * sizeof(unsigned long long)));
+        CK(dalloc(ctx, &ctx->wkeys_sorted, n * sizeof(unsigned long long)));
+        CK(dalloc(ctx, &ctx->wvals, n * sizeof(int)));
+        CK(dalloc(ctx, &ctx->order, n * sizeof(int)));
+        CK(dalloc(ctx, &ctx->small, 16 * sizeof(int)));
+        CK(dalloc(ctx, &ctx->score_acc, sizeof(unsigned long long)));
+        CK(dalloc(ctx, &ctx->cstats, sizeof(CommitStats)));
+        size_t b1 = 0, b2 = 0;
+        CK(cub::DeviceRadixSort::SortKeys(nullptr, b1, ctx->ckeys, ctx->ckeys_sorted, n));
+        CK(cub::DeviceRadixSort::SortPairsDescending(nullptr, b2, ctx->wkeys, ctx->wkeys_sorted,
+                                                     ctx->wvals, ctx->order, n));
+        ctx->cub_bytes = std::max(b1, b2);
+        CK(dalloc(ctx, &ctx->cub_tmp, ctx->cub_bytes));
+        CK(cudaDeviceSynchronize());
+        return BM_OK;
+    };
+    bm_status s = body();
+    if (s != BM_OK) return fail(s);
+    *out = ctx;
+    return BM_OK;
+}
+
+extern "C" bm_status bm_get_info(const bm_ctx* ctx, bm_info* info) {
+    if (!ctx || !info) return BM_E_INPUT;
+    info->n = ctx->n;
+    info->entry_bits = ctx->w16 ? 16 : 32;
+    info->e1 = ctx->e1;
+    info->e2 = ctx->e2;
+    info->g1_self_loops = ctx->nself;
+    info->device_bytes = ctx->dev_bytes;
+    info->device = ctx->dev;
+    info->num_sms = ctx->num_sms;
+    return BM_OK;
+}
+
+// ---------------------------------------------------------------------------
+static bm_status compute_score(bm_ctx* ctx, long long* out) {
+    CK(cudaMemsetAsync(ctx->score_acc, 0, sizeof(unsigned long long), ctx->st));
+    const int blocks = ctx->num_sms * 4;
+    if (ctx->w16) k_score<true><<<blocks, 256, 0, ctx->st>>>(view<true>(ctx), ctx->score_acc);
+    else k_score<false><<<blocks, 256, 0, ctx->st>>>(view<false>(ctx), ctx->score_acc);
+    CK(cudaGetLastError());
+    unsigned long long v = 0;
+    CK(cudaMemcpyAsync(&v, ctx->score_acc, sizeof v, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    *out = (long long)v;
+    return BM_OK;
+}
+
+extern "C" bm_status bm_set_mapping(bm_ctx* ctx, const int32_t* map) {
+    if (!ctx) return BM_E_INPUT;
+    if (!map) { set_err(ctx, "bm_set_mapping: map is NULL"); return BM_E_INPUT; }
+    const int n = ctx->n;
+    std::vector<int> p(n + 1), pinv(n + 1, n);
+    for (int a = 0; a < n; a++) {
+        const int f = map[a + 1];
+        if (f < 0 || f > n) { set_err(ctx, "bm_set_mapping: map[%d]=%d outside 0..%d", a + 1, f, n); return BM_E_INPUT; }
+        if (f == 0) { p[a] = n; continue; }
+        if (pinv[f - 1] != n) { set_err(ctx, "bm_set_mapping: G2 vertex %d matched twice (m%d and m%d)", f, pinv[f - 1] + 1, a + 1); return BM_E_INPUT; }
+        p[a] = f - 1;
+        pinv[f - 1] = a;
+    }
+    p[n] = n;
+    pinv[n] = n;
+    CK(cudaMemcpyAsync(ctx->p, p.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->pinv, pinv.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+    ctx->mapped = true;
+    return compute_score(ctx, &ctx->score);
+}
+
+extern "C" bm_status bm_get_mapping(bm_ctx* ctx, int32_t* map) {
+    if (!ctx || !map) return BM_E_INPUT;
+    if (!ctx->mapped) { set_err(ctx, "bm_get_mapping: no mapping set"); return BM_E_STATE; }
+    const int n = ctx->n;
+    std::vector<int> p(n + 1);
+    CK(cudaMemcpyAsync(p.data(), ctx->p, (n + 1) * sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    map[0] = 0;
+    for (int a = 0; a < n; a++) map[a + 1] = p[a] == n ? 0 : p[a] + 1;
+    return BM_OK;
+}
+
+extern "C" bm_status bm_score(bm_ctx* ctx, int64_t* score) {
+    if (!ctx || !score) return BM_E_INPUT;
+    if (!ctx->mapped) { set_err(ctx, "bm_score: no mapping set"); return BM_E_STATE; }
+    long long s = 0;
+    bm_status r = compute_score(ctx, &s);
+    if (r) return r;
+    *score = s;
+    return BM_OK;
+}
+
+static bm_status ensure_scratch(bm_ctx* ctx, long long ints) {
+    if (ints <= ctx->scratch_cap) return BM_OK;
+    if (ctx->scratch_pairs) { cudaFree(ctx->scratch_pairs); ctx->dev_bytes -= ctx->scratch_cap * (long long)sizeof(int); }
+    ctx->scratch_pairs = nullptr;
+    ctx->scratch_cap = 0;
+    CK(dalloc(ctx, &ctx->scratch_pairs, (size_t)ints * sizeof(int)));
+    ctx->scratch_cap = ints;
+    return BM_OK;
+}
+
+extern "C" bm_status bm_pair_deltas(bm_ctx* ctx, int64_t k, const int32_t* m1, const int32_t* m2,
+                                    int32_t* out) {
+    if (!ctx) return BM_E_INPUT;
+    if (!ctx->mapped) { set_err(ctx, "bm_pair_deltas: no mapping set"); return BM_E_STATE; }
+    if (k < 0 || (k && (!m1 || !m2 || !out))) { set_err(ctx, "bm_pair_deltas: bad arguments"); return BM_E_INPUT; }
+    if (k == 0) return BM_OK;
+    const int n = ctx->n;
+    std::vector<int> a(k), b(k);
+    for (int64_t i = 0; i < k; i++) {
+        if (m1[i] < 1 || m1[i] > n || m2[i] < 1 || m2[i] > n || m1[i] == m2[i]) {
+            set_err(ctx, "bm_pair_deltas: pair %lld = (%d,%d) invalid", (long long)i, m1[i], m2[i]);
+            return BM_E_INPUT;
+        }
+        a[i] = m1[i] - 1;
+        b[i] = m2[i] - 1;
+    }
+    bm_status s = ensure_scratch(ctx, 3 * k);
+    if (s) return s;
+    int* da = ctx->scratch_pairs;
+    int* db = da + k;
+    int* dout = db + k;
+    CK(cudaMemcpyAsync(da, a.data(), k * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(db, b.data(), k * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+    const long long blocks = std::min<long long>((k + 7) / 8, (long long)ctx->num_sms * 16);
+    if (ctx->w16) k_pair_deltas<true><<<(int)blocks, 256, 0, ctx->st>>>(view<true>(ctx), da, db, k, dout);
+    else k_pair_deltas<false><<<(int)blocks, 256, 0, ctx->st>>>(view<false>(ctx), da, db, k, dout);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, dout, k * sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return BM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Sweep stages.
+static bm_status ensure_S(bm_ctx* ctx) {
+    if (ctx->S) return BM_OK;
+    CK(dalloc(ctx, &ctx->S, (size_t)ctx->n * ctx->n * sizeof(int)));
+    return BM_OK;
+}
+
+template <bool W16>
+static bm_status stage_profit(bm_ctx* ctx) {
+    typedef typename Ent<W16>::T E;
+    DevView<W16> g = view<W16>(ctx);
+    const int n = ctx->n;
+    const int rb = ctx->num_sms * 8;
+    k_relabel<W16><<<rb, 256, 0, ctx->st>>>((const E*)ctx->ent1o, (E*)ctx->ent1oP, ctx->e1, ctx->p);
+    k_relabel<W16><<<rb, 256, 0, ctx->st>>>((const E*)ctx->ent1i, (E*)ctx->ent1iP, ctx->e1, ctx->p);
+    k_relabel<W16><<<rb, 256, 0, ctx->st>>>((const E*)ctx->ent2o, (E*)ctx->ent2oP, ctx->e2, ctx->pinv);
+    k_relabel<W16><<<rb, 256, 0, ctx->st>>>((const E*)ctx->ent2i, (E*)ctx->ent2iP, ctx->e2, ctx->pinv);
+    CK(cudaGetLastError());
+    // heaviest rows first
+    CK(cudaMemsetAsync(ctx->work_sum, 0, sizeof(unsigned long long), ctx->st));
+    k_row_work<W16><<<(n + 7) / 8, 256, 0, ctx->st>>>(g, ctx->wkeys, ctx->wvals, ctx->work_sum);
+    CK(cudaGetLastError());
+    size_t tb = ctx->cub_bytes;
+    CK(cub::DeviceRadixSort::SortPairsDescending(ctx->cub_tmp, tb, ctx->wkeys, ctx->wkeys_sorted,
+                                                 ctx->wvals, ctx->order, n, 0, 64, ctx->st));
+    CK(cudaMemsetAsync(ctx->small, 0, sizeof(int), ctx->st));
+    const size_t smem = (size_t)(n + 1) * sizeof(int);
+    CK(cudaFuncSetAttribute(k_profit<W16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_profit<W16>, 512, smem));
+    if (per_sm < 1) { set_err(ctx, "profit kernel does not fit (n=%d)", n); return BM_E_INPUT; }
+    CK(cudaEventRecord(ctx->ev[4], ctx->st));
+    k_profit<W16><<<ctx->num_sms * per_sm, 512, smem, ctx->st>>>(g, ctx->order, ctx->small);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ctx->ev[5], ctx->st));
+    return BM_OK;
+}
+
+static bm_status stage_combine(bm_ctx* ctx, int* all_out) {
+    const int n = ctx->n;
+    CK(cudaMemsetAsync(ctx->rowbest, 0, n * sizeof(unsigned long long), ctx->st));
+    const int t = (n + 31) / 32;
+    dim3 grid(t, t), block(32, 8);
+    k_combine<<<grid, block, 0, ctx->st>>>(ctx->S, n, ctx->rowbest, all_out);
+    CK(cudaGetLastError());
+    return BM_OK;
+}
+
+template <bool W16>
+static bm_status stage_commit(bm_ctx* ctx, const bm_sweep_opts* o) {
+    const int n = ctx->n;
+    CK(cudaMemsetAsync(ctx->small + 1, 0, 2 * sizeof(int), ctx->st));
+    k_candidates<<<(n + 255) / 256, 256, 0, ctx->st>>>(ctx->rowbest, n, ctx->ckeys, ctx->small + 1, ctx->small + 2);
+    CK(cudaGetLastError());
+    size_t tb = ctx->cub_bytes;
+    CK(cub::DeviceRadixSort::SortKeys(ctx->cub_tmp, tb, ctx->ckeys, ctx->ckeys_sorted, n, 0, 64, ctx->st));
+    const size_t smem = 2 * (size_t)n;
+    CK(cudaFuncSetAttribute(k_commit<W16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int max_scan = o ? o->max_candidates : 0;
+    const int max_verify = o ? o->max_verify : -1;
+    k_commit<W16><<<1, 1024, smem, ctx->st>>>(view<W16>(ctx), ctx->ckeys_sorted, n, max_scan, max_verify,
+                                               ctx->cstats, nullptr);
+    CK(cudaGetLastError());
+    return BM_OK;
+}
+
+extern "C" bm_status bm_all_deltas(bm_ctx* ctx, int32_t* out) {
+    if (!ctx || !out) return BM_E_INPUT;
+    if (!ctx->mapped) { set_err(ctx, "bm_all_deltas: no mapping set"); return BM_E_STATE; }
+    bm_status s = ensure_S(ctx);
+    if (s) return s;
+    const long long np = (long long)ctx->n * (ctx->n - 1) / 2;
+    int* d = nullptr;
+    CK(cudaMalloc(&d, np * sizeof(int)));
+    s = ctx->w16 ? stage_profit<true>(ctx) : stage_profit<false>(ctx);
+    if (!s) s = stage_combine(ctx, d);
+    if (!s) {
+        cudaError_t e = cudaMemcpyAsync(out, d, np * sizeof(int), cudaMemcpyDeviceToHost, ctx->st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->st);
+        if (e != cudaSuccess) { set_err(ctx, "bm_all_deltas: %s", cudaGetErrorString(e)); s = BM_E_CUDA; }
+    }
+    cudaFree(d);
+    return s;
+}
+
+extern "C" bm_status bm_profit_row(bm_ctx* ctx, int32_t a, int32_t* out) {
+    if (!ctx || !out) return BM_E_INPUT;
+    if (!ctx->mapped) { set_err(ctx, "bm_profit_row: no mapping set"); return BM_E_STATE; }
+    if (a < 1 || a > ctx->n) { set_err(ctx, "bm_profit_row: a=%d outside 1..%d", a, ctx->n); return BM_E_INPUT; }
+    bm_status s = ensure_S(ctx);
+    if (s) return s;
+    s = ctx->w16 ? stage_profit<true>(ctx) : stage_profit<false>(ctx);
+    if (s) return s;
+    CK(cudaMemcpyAsync(out, ctx->S + (size_t)(a - 1) * ctx->n, ctx->n * sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return BM_OK;
+}
+
+extern "C" bm_status bm_sweep(bm_ctx* ctx, const bm_sweep_opts* opts, bm_sweep_stats* stats) {
+    if (!ctx) return BM_E_INPUT;
+    if (!ctx->mapped) { set_err(ctx, "bm_sweep: no mapping set"); return BM_E_STATE; }
+    bm_status s = ensure_S(ctx);
+    if (s) return s;
+    const long long before = ctx->score;
+    CK(cudaEventRecord(ctx->ev[0], ctx->st));
+    s = ctx->w16 ? stage_profit<true>(ctx) : stage_profit<false>(ctx);
+    if (s) return s;
+    CK(cudaEventRecord(ctx->ev[1], ctx->st));
+    s = stage_combine(ctx, nullptr);
+    if (s) return s;
+    CK(cudaEventRecord(ctx->ev[2], ctx->st));
+    s = ctx->w16 ? stage_commit<true>(ctx, opts) : stage_commit<false>(ctx, opts);
+    if (s) return s;
+    CK(cudaEventRecord(ctx->ev[3], ctx->st));
+    CommitStats cs;
+    int small[3];
+    unsigned long long terms = 0;
+    CK(cudaMemcpyAsync(&cs, ctx->cstats, sizeof cs, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(small, ctx->small, 3 * sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(&terms, ctx->work_sum, sizeof terms, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    ctx->score = before + cs.total_delta;
+    if (stats) {
+        memset(stats, 0, sizeof *stats);
+        stats->score_before = before;
+        stats->score_after = ctx->score;
+        stats->deltas_evaluated = (long long)ctx->n * (ctx->n - 1) / 2;
+        stats->candidates = small[1];
+        stats->best_delta = small[2];
+        stats->scanned = cs.scanned;
+        stats->verified = cs.verified;
+        stats->committed = cs.committed;
+        cudaEventElapsedTime(&stats->ms_prep, ctx->ev[0], ctx->ev[4]);
+        cudaEventElapsedTime(&stats->ms_profit, ctx->ev[4], ctx->ev[5]);
+        cudaEventElapsedTime(&stats->ms_combine, ctx->ev[1], ctx->ev[2]);
+        cudaEventElapsedTime(&stats->ms_commit, ctx->ev[2], ctx->ev[3]);
+        cudaEventElapsedTime(&stats->ms_total, ctx->ev[0], ctx->ev[3]);
+        stats->min_terms = (long long)terms;
+    }
+    return BM_OK;
+}
+
+extern "C" bm_status bm_timer_mark(bm_ctx* ctx, int32_t slot) {
+    if (!ctx || slot < 0 || slot >= 8) return BM_E_INPUT;
+    CK(cudaEventRecord(ctx->uev[slot], ctx->st));
+    return BM_OK;
+}
+
+extern "C" bm_status bm_timer_elapsed(bm_ctx* ctx, int32_t a, int32_t b, float* ms) {
+    if (!ctx || !ms || a < 0 || a >= 8 || b < 0 || b >= 8) return BM_E_INPUT;
+    CK(cudaEventSynchronize(ctx->uev[b]));
+    CK(cudaEventElapsedTime(ms, ctx->uev[a], ctx->uev[b]));
+    return BM_OK;
+}
+
+extern "C" bm_status bm_hillclimb(bm_ctx* ctx, int32_t max_sweeps, const bm_sweep_opts* opts,
+                                  bm_sweep_stats* per_sweep, int32_t* sweeps_done) {
+    if (!ctx || max_sweeps < 0) return BM_E_INPUT;
+    int done = 0;
+    for (; done < max_sweeps; done++) {
+        bm_sweep_stats st;
+        bm_status s = bm_sweep(ctx, opts, &st);
+        if (s) { if (sweeps_done) *sweeps_done = done; return s; }
+        if (per_sweep) per_sweep[done] = st;
+        if (st.committed == 0) { done++; break; }
+    }
+    if (sweeps_done) *sweeps_done = done;
+    return BM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Reference-order first improvement (src/graph-alignment-optimized.c:515-577).
+__global__ void k_first_reset(int* first, int n) { first[0] = n; }
+__global__ void k_first_publish(int* first, int n) { first[1] = first[0]; first[0] = n; }
+
+template <bool W16>
+static bm_status first_improvement_impl(bm_ctx* ctx, int max_passes, long long* commits, int* passes) {
+    const int n = ctx->n;
+    if (!ctx->rowd) CK(dalloc(ctx, &ctx->rowd, n * sizeof(int)));
+    if (!ctx->first) CK(dalloc(ctx, &ctx->first, 2 * sizeof(int)));
+    if (!ctx->fi_acc) CK(dalloc(ctx, &ctx->fi_acc, 2 * sizeof(long long)));
+    CK(cudaMemsetAsync(ctx->fi_acc, 0, 2 * sizeof(long long), ctx->st));
+    k_first_reset<<<1, 1, 0, ctx->st>>>(ctx->first, n);
+    DevView<W16> g = view<W16>(ctx);
+    long long total = 0;
+    int pass = 0;
+    const int blocks = std::min((n + 7) / 8, ctx->num_sms * 16);
+    for (; pass < max_passes; pass++) {
+        long long in_pass = 0;
+        for (int m1 = 0; m1 < n; m1++) {
+            int start = 0;
+            while (start < n) {
+                k_row_first<W16><<<blocks, 256, 0, ctx->st>>>(g, m1, start, ctx->rowd, ctx->first);
+                k_apply_first<<<1, 1, 0, ctx->st>>>(ctx->p, ctx->pinv, n, m1, ctx->first, ctx->rowd, ctx->fi_acc);
+                k_first_publish<<<1, 1, 0, ctx->st>>>(ctx->first, n);
+                CK(cudaGetLastError());
+                int m2 = n;
+                CK(cudaMemcpyAsync(&m2, ctx->first + 1, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+                CK(cudaStreamSynchronize(ctx->st));
+                if (m2 >= n) break;
+                in_pass++;
+                start = m2 + 1;
+            }
+        }
+        total += in_pass;
+        if (in_pass == 0) { pass++; break; }
+    }
+    long long acc[2] = {0, 0};
+    CK(cudaMemcpyAsync(acc, ctx->fi_acc, sizeof acc, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    ctx->score += acc[0];
+    *commits = total;
+    *passes = pass;
+    return BM_OK;
+}
+
+extern "C" bm_status bm_first_improvement(bm_ctx* ctx, int32_t max_passes, int64_t* commits,
+                                          int32_t* passes_done) {
+    if (!ctx || max_passes < 0) return BM_E_INPUT;
+    if (!ctx->mapped) { set_err(ctx, "bm_first_improvement: no mapping set"); return BM_E_STATE; }
+    long long c = 0;
+    int p = 0;
+    bm_status s = ctx->w16 ? first_improvement_impl<true>(ctx, max_passes, &c, &p)
+                           : first_improvement_impl<false>(ctx, max_passes, &c, &p);
+    if (commits) *commits = c;
+    if (passes_done) *passes_done = p;
+    return s;
+}
+
+// ---------------------------------------------------------------------------
+// 3-cycles.
+extern "C" bm_status bm_triple_deltas(bm_ctx* ctx, int64_t k, const int32_t* a, const int32_t* b,
+                                      const int32_t* c, int32_t* out) {
+    if (!ctx) return BM_E_INPUT;
+    if (!ctx->mapped) { set_err(ctx, "bm_triple_deltas: no mapping set"); return BM_E_STATE; }
+    if (k < 0 || (k && (!a || !b || !c || !out))) { set_err(ctx, "bm_triple_deltas: bad arguments"); return BM_E_INPUT; }
+    if (k == 0) return BM_OK;
+    const int n = ctx->n;
+    std::vector<int> h(3 * k);
+    for (int64_t i = 0; i < k; i++) {
+        const int x = a[i], y = b[i], z = c[i];
+        if (x < 1 || x > n || y < 1 || y > n || z < 1 || z > n || x == y || y == z || x == z) {
+            set_err(ctx, "bm_triple_deltas: triple %lld = (%d,%d,%d) invalid", (long long)i, x, y, z);
+            return BM_E_INPUT;
+        }
+        h[i] = x - 1; h[k + i] = y - 1; h[2 * k + i] = z - 1;
+    }
+    bm_status s = ensure_scratch(ctx, 5 * k);
+    if (s) return s;
+    int* d = ctx->scratch_pairs;
+    CK(cudaMemcpyAsync(d, h.data(), 3 * k * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+    const long long blocks = std::min<long long>((k + 7) / 8, (long long)ctx->num_sms * 16);
+    if (ctx->w16) k_triple_deltas<true><<<(int)blocks, 256, 0, ctx->st>>>(view<true>(ctx), d, d + k, d + 2 * k, k, d + 3 * k);
+    else k_triple_deltas<false><<<(int)blocks, 256, 0, ctx->st>>>(view<false>(ctx), d, d + k, d + 2 * k, k, d + 3 * k);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, d + 3 * k, 2 * k * sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return BM_OK;
+}
+
+template <bool W16>
+static bm_status triple_round_impl(bm_ctx* ctx, const bm_triple_opts* o, bm_triple_stats* stats) {
+    const int n = ctx->n;
+    const int partners = o->partners > 0 ? o->partners : 256;
+    if (partners > 32768) { set_err(ctx, "bm_triple_round: partners=%d above 32768", partners); return BM_E_INPUT; }
+    bm_status s = ensure_S(ctx);
+    if (s) return s;
+    if (!ctx->adj) {
+        ctx->adj_words = (n + 31) / 32;
+        const size_t bytes = (size_t)n * ctx->adj_words * sizeof(unsigned);
+        CK(dalloc(ctx, &ctx->adj, bytes));
+        CK(cudaMemsetAsync(ctx->adj, 0, bytes, ctx->st));
+        k_adj_bits<W16><<<(n + 7) / 8, 256, 0, ctx->st>>>(view<W16>(ctx), ctx->adj, ctx->adj_words);
+        CK(cudaGetLastError());
+    }
+    if (!ctx->tcount) CK(dalloc(ctx, &ctx->tcount, 2 * sizeof(unsigned long long)));
+    const long long before = ctx->score;
+    CK(cudaEventRecord(ctx->ev[0], ctx->st));
+    s = stage_profit<W16>(ctx);
+    if (s) return s;
+    CK(cudaEventRecord(ctx->ev[1], ctx->st));
+    CK(cudaMemsetAsync(ctx->tcount, 0, 2 * sizeof(unsigned long long), ctx->st));
+    const int blocks = std::min(n, ctx->num_sms * 8);
+    k_triple_eval<W16><<<blocks, 256, 0, ctx->st>>>(view<W16>(ctx), ctx->adj, ctx->adj_words, partners,
+                                                    o->seed, ctx->ckeys, ctx->tcount);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ctx->ev[2], ctx->st));
+    size_t tb = ctx->cub_bytes;
+    CK(cub::DeviceRadixSort::SortKeys(ctx->cub_tmp, tb, ctx->ckeys, ctx->ckeys_sorted, n, 0, 64, ctx->st));
+    const size_t smem = 2 * (size_t)n;
+    CK(cudaFuncSetAttribute(k_triple_commit<W16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_triple_commit<W16><<<1, 1024, smem, ctx->st>>>(view<W16>(ctx), ctx->ckeys_sorted, n, o->max_candidates,
+                                                      o->max_verify, o->seed, ctx->cstats);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ctx->ev[3], ctx->st));
+    CommitStats cs;
+    unsigned long long cnt[2];
+    std::vector<unsigned long long> keys(n);
+    CK(cudaMemcpyAsync(&cs, ctx->cstats, sizeof cs, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(cnt, ctx->tcount, sizeof cnt, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(keys.data(), ctx->ckeys_sorted, n * sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    ctx->score = before + cs.total_delta;
+    if (stats) {
+        memset(stats, 0, sizeof *stats);
+        stats->score_before = before;
+        stats->score_after = ctx->score;
+        stats->triples = (long long)cnt[0];
+        stats->rotations = 2 * (long long)cnt[0];
+        int nc = 0;
+        while (nc < n && keys[nc] != ~0ull) nc++;
+        stats->candidates = nc;
+        stats->best_delta = nc ? (int)(0x7fffffffu - (unsigned)(keys[0] >> 32)) : 0;
+        stats->scanned = cs.scanned;
+        stats->verified = cs.verified;
+        stats->committed = cs.committed;
+        cudaEventElapsedTime(&stats->ms_sample, ctx->ev[0], ctx->ev[1]);
+        cudaEventElapsedTime(&stats->ms_eval, ctx->ev[1], ctx->ev[2]);
+        cudaEventElapsedTime(&stats->ms_commit, ctx->ev[2], ctx->ev[3]);
+        cudaEventElapsedTime(&stats->ms_total, ctx->ev[0], ctx->ev[3]);
+    }
+    return BM_OK;
+}
+
+extern "C" bm_status bm_triple_round(bm_ctx* ctx, const bm_triple_opts* opts, bm_triple_stats* stats) {
+    if (!ctx || !opts) return BM_E_INPUT;
+    if (!ctx->mapped) { set_err(ctx, "bm_triple_round: no mapping set"); return BM_E_STATE; }
+    return ctx->w16 ? triple_round_impl<true>(ctx, opts, stats) : triple_round_impl<false>(ctx, opts, stats);
+}

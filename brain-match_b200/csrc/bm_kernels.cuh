@@ -1,0 +1,478 @@
+// bm_kernels.cuh -- sm_100a device code of the swap-delta engine.
+//
+// Notation (0-based inside the engine; the C ABI is 1-based like the
+// reference):  G1 vertices a,b,u,v in [0,n);  G2 vertices f,g in [0,n);
+// p: G1 -> G2 (value n = unmatched, "NONE");  pinv: G2 -> G1 (n = NONE).
+// W2 is G2's dense (n+1)x(n+1) weight matrix whose row and column n are 0,
+// which plays the role of the reference's unused row/column 0.
+//
+// Profit matrix.  For every ordered pair (a,b) of G1 vertices
+//     S[a][b] = sum_{(a,v,w) in out1(a)} min(w, W2[p b][p v])
+//             + sum_{(u,a,w) in in1(a)}  min(w, W2[p u][p b])
+//             + unary self-loop terms + per-edge corner corrections
+// i.e. the score a would earn by taking p(b) while everyone else stays.
+// S[a][a] is a's current contribution, and the exact swap delta is
+//     delta(a,b) = S[a][b] + S[b][a] - S[a][a] - S[b][b]
+// once the corner corrections below are folded into S.  This is the same
+// arithmetic as calculate_swap_delta (src/graph-alignment-optimized.c:321-408)
+// regrouped by row: the reference skips the partner in each edge list and adds
+// the two a<->b edges separately; here those terms are removed or replaced by
+// the correction  min(x,W2[pa][pb]) + min(x,W2[pb][pa]) - min(x,W2[pa][pa])
+// - min(x,W2[pb][pb])  added to S[a][b] for every G1 edge a->b of weight x.
+//
+// S is accumulated sparse x sparse: for each out-edge (a,v,w1) of a, every
+// G2 in-edge (g -> p(v), w2) contributes min(w1,w2) to S[a][pinv(g)]; for each
+// in-edge (u,a,w1), every G2 out-edge (p(u) -> g, w2) contributes to
+// S[a][pinv(g)].  Only nonzero min terms are ever touched.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace bm {
+
+// ---- list entries: (id, weight) packed per storage mode ----
+template <bool W16> struct Ent;
+template <> struct Ent<true> {
+    typedef uint32_t T;  // id in bits 0..15, weight in bits 16..31
+    static __host__ __device__ __forceinline__ int id(T e) { return (int)(e & 0xFFFFu); }
+    static __host__ __device__ __forceinline__ int w(T e) { return (int)(e >> 16); }
+    static __host__ __device__ __forceinline__ T make(int i, int w) { return (uint32_t)i | ((uint32_t)w << 16); }
+};
+template <> struct Ent<false> {
+    typedef int2 T;  // x = id, y = weight
+    static __host__ __device__ __forceinline__ int id(T e) { return e.x; }
+    static __host__ __device__ __forceinline__ int w(T e) { return e.y; }
+    static __host__ __device__ __forceinline__ T make(int i, int w) { return make_int2(i, w); }
+};
+template <bool W16> struct Dense;
+template <> struct Dense<true> { typedef uint16_t T; };
+template <> struct Dense<false> { typedef int32_t T; };
+
+// Device view of a context.
+template <bool W16> struct DevView {
+    typedef typename Ent<W16>::T E;
+    typedef typename Dense<W16>::T D;
+    int n;
+    const int* off1o; const E* ent1o;   // G1 out-lists (id = dst)
+    const int* off1i; const E* ent1i;   // G1 in-lists  (id = src)
+    const int* off2o; const E* ent2o;   // G2 out-lists (id = dst)
+    const int* off2i; const E* ent2i;   // G2 in-lists  (id = src)
+    const int* offs;  const int* selfw; // G1 self-loops per vertex
+    E* ent1oP; E* ent1iP;               // G1 lists with ids mapped through p
+    E* ent2oP; E* ent2iP;               // G2 lists with ids mapped through pinv
+    const D* W2;                        // dense (n+1)^2, row/col n zero
+    int* p; int* pinv;                  // n+1 entries, [n] = n
+    int* S;                             // n*n profit matrix
+    __device__ __forceinline__ int w2(int f, int g) const {
+        return (int)W2[(size_t)f * (size_t)(n + 1) + (size_t)g];
+    }
+};
+
+__device__ __forceinline__ int imin(int a, int b) { return a < b ? a : b; }
+
+// ---------------------------------------------------------------------------
+// Relabel list ids through a map (p for G1 lists, pinv for G2 lists).
+template <bool W16>
+__global__ void k_relabel(const typename Ent<W16>::T* __restrict__ in,
+                          typename Ent<W16>::T* __restrict__ out, long long m,
+                          const int* __restrict__ map) {
+    typedef Ent<W16> EN;
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long stride = (long long)gridDim.x * blockDim.x;
+    for (; i < m; i += stride) {
+        typename EN::T e = in[i];
+        out[i] = EN::make(__ldg(&map[EN::id(e)]), EN::w(e));
+    }
+}
+
+// Work estimate of a profit row: number of min terms it scatters.
+template <bool W16>
+__global__ void k_row_work(DevView<W16> g, unsigned long long* __restrict__ key,
+                           int* __restrict__ val, unsigned long long* __restrict__ total) {
+    typedef Ent<W16> EN;
+    const int lane = threadIdx.x & 31;
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int a = warp; a < g.n; a += nwarps) {
+        long long w = 0;
+        for (int i = g.off1o[a] + lane; i < g.off1o[a + 1]; i += 32) {
+            int f = EN::id(g.ent1oP[i]);
+            w += g.off2i[f + 1] - g.off2i[f];
+        }
+        for (int i = g.off1i[a] + lane; i < g.off1i[a + 1]; i += 32) {
+            int f = EN::id(g.ent1iP[i]);
+            w += g.off2o[f + 1] - g.off2o[f];
+        }
+        for (int o = 16; o; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+        if (lane == 0) {
+            atomicAdd(total, (unsigned long long)w);   // min terms the row scatters
+            w += (g.off1o[a + 1] - g.off1o[a]) + (g.off1i[a + 1] - g.off1i[a]);
+            if (g.offs[a + 1] > g.offs[a]) w += g.n;
+            key[a] = (unsigned long long)w;
+            val[a] = a;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Profit rows.  Persistent CTAs take rows from `order` (heaviest first) via an
+// atomic counter, accumulate the row in shared memory (n+1 ints: slot n
+// absorbs terms for unmatched G2 vertices) and write it to S[a][0..n).
+template <bool W16>
+__global__ void __launch_bounds__(512)
+k_profit(DevView<W16> g, const int* __restrict__ order, int* __restrict__ counter) {
+    typedef Ent<W16> EN;
+    typedef typename EN::T E;
+    extern __shared__ int acc[];
+    __shared__ int s_row;
+    const int n = g.n;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+    for (;;) {
+        if (tid == 0) s_row = atomicAdd(counter, 1);
+        __syncthreads();
+        const int r = s_row;
+        if (r >= n) break;
+        const int a = order[r];
+        for (int i = tid; i <= n; i += blockDim.x) acc[i] = 0;
+        __syncthreads();
+        // out-edges of a against G2 in-lists of p(v)
+        {
+            const int s0 = g.off1o[a], s1 = g.off1o[a + 1];
+            for (int j = s0 + wid; j < s1; j += nw) {
+                const E ea = g.ent1oP[j];
+                const int f = EN::id(ea), w1 = EN::w(ea);
+                const int b0 = g.off2i[f], b1 = g.off2i[f + 1];
+                int i = b0 + lane;
+                for (; i + 32 < b1; i += 64) {
+                    const E x = g.ent2iP[i], y = g.ent2iP[i + 32];
+                    atomicAdd(&acc[EN::id(x)], imin(w1, EN::w(x)));
+                    atomicAdd(&acc[EN::id(y)], imin(w1, EN::w(y)));
+                }
+                if (i < b1) { const E x = g.ent2iP[i]; atomicAdd(&acc[EN::id(x)], imin(w1, EN::w(x))); }
+            }
+        }
+        // in-edges of a against G2 out-lists of p(u)
+        {
+            const int s0 = g.off1i[a], s1 = g.off1i[a + 1];
+            for (int j = s0 + wid; j < s1; j += nw) {
+                const E ea = g.ent1iP[j];
+                const int f = EN::id(ea), w1 = EN::w(ea);
+                const int b0 = g.off2o[f], b1 = g.off2o[f + 1];
+                int i = b0 + lane;
+                for (; i + 32 < b1; i += 64) {
+                    const E x = g.ent2oP[i], y = g.ent2oP[i + 32];
+                    atomicAdd(&acc[EN::id(x)], imin(w1, EN::w(x)));
+                    atomicAdd(&acc[EN::id(y)], imin(w1, EN::w(y)));
+                }
+                if (i < b1) { const E x = g.ent2oP[i]; atomicAdd(&acc[EN::id(x)], imin(w1, EN::w(x))); }
+            }
+        }
+        // corner corrections for every G1 edge a->b
+        {
+            const int pa = g.p[a];
+            const int s0 = g.off1o[a], s1 = g.off1o[a + 1];
+            for (int j = s0 + tid; j < s1; j += blockDim.x) {
+                const int b = EN::id(g.ent1o[j]);
+                const E ep = g.ent1oP[j];
+                const int pb = EN::id(ep), x = EN::w(ep);
+                const int c = imin(x, g.w2(pa, pb)) + imin(x, g.w2(pb, pa))
+                            - imin(x, g.w2(pa, pa)) - imin(x, g.w2(pb, pb));
+                if (c) atomicAdd(&acc[b], c);
+            }
+        }
+        // unary terms of G1 self-loops: a taking p(b) earns min(s, W2[p b][p b])
+        {
+            const int q0 = g.offs[a], q1 = g.offs[a + 1];
+            if (q1 > q0) {
+                for (int b = tid; b < n; b += blockDim.x) {
+                    const int pb = g.p[b];
+                    const int d = g.w2(pb, pb);
+                    int t = 0;
+                    for (int q = q0; q < q1; q++) t += imin(g.selfw[q], d);
+                    acc[b] += t;
+                }
+            }
+        }
+        __syncthreads();
+        int* row = g.S + (size_t)a * (size_t)n;
+        if ((n & 3) == 0) {
+            int4* r4 = reinterpret_cast<int4*>(row);
+            const int4* a4 = reinterpret_cast<const int4*>(acc);
+            for (int i = tid; i < (n >> 2); i += blockDim.x) r4[i] = a4[i];
+        } else {
+            for (int i = tid; i < n; i += blockDim.x) row[i] = acc[i];
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Pair combine.  32x32 tiles of the upper triangle: delta(a,b) for a<b from
+// S[a][b], S[b][a] and the diagonal.  Keeps, per row, the best partner as a
+// packed key  (delta + 2^31) << 32 | ~b  (larger delta, then smaller b, wins)
+// and optionally writes every delta at the reference's linear pair index.
+__device__ __forceinline__ unsigned long long pack_best(int d, int b) {
+    return ((unsigned long long)(unsigned)(d + 0x80000000u) << 32) | (unsigned)(~b);
+}
+__device__ __forceinline__ unsigned long long kmax(unsigned long long x, unsigned long long y) {
+    return x > y ? x : y;
+}
+
+__global__ void __launch_bounds__(256)
+k_combine(const int* __restrict__ S, int n, unsigned long long* __restrict__ rowbest,
+          int* __restrict__ all_out) {
+    __shared__ int sA[32][33];  // S[a0+r][b0+c]
+    __shared__ int sB[32][33];  // S[b0+r][a0+c]
+    __shared__ int dA[32], dB[32];
+    __shared__ unsigned long long colbest[8][32];
+    const int ti = blockIdx.y, tj = blockIdx.x;
+    if (ti > tj) return;
+    const int a0 = ti * 32, b0 = tj * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    for (int r = ty; r < 32; r += 8) {
+        const int a = a0 + r, b = b0 + tx;
+        sA[r][tx] = (a < n && b < n) ? S[(size_t)a * n + b] : 0;
+        const int bb = b0 + r, aa = a0 + tx;
+        sB[r][tx] = (bb < n && aa < n) ? S[(size_t)bb * n + aa] : 0;
+    }
+    if (ty == 0) {
+        const int a = a0 + tx, b = b0 + tx;
+        dA[tx] = a < n ? S[(size_t)a * n + a] : 0;
+        dB[tx] = b < n ? S[(size_t)b * n + b] : 0;
+    }
+    __syncthreads();
+    const int b = b0 + tx;
+    unsigned long long cb = 0;  // best partner a for row b
+    for (int r = ty; r < 32; r += 8) {
+        const int a = a0 + r;
+        const bool ok = (a < b) && (b < n);
+        int d = 0;
+        if (ok) {
+            d = sA[r][tx] + sB[tx][r] - dA[r] - dB[tx];
+            if (all_out) {
+                const long long idx = (long long)a * (2LL * n - a - 1) / 2 + (b - a - 1);
+                all_out[idx] = d;
+            }
+            cb = kmax(cb, pack_best(d, a));
+        }
+        unsigned long long rk = ok ? pack_best(d, b) : 0ull;
+        for (int o = 16; o; o >>= 1) rk = kmax(rk, __shfl_xor_sync(0xffffffffu, rk, o));
+        if (tx == 0 && rk) atomicMax(&rowbest[a], rk);
+    }
+    colbest[ty][tx] = cb;
+    __syncthreads();
+    if (ty == 0) {
+        unsigned long long k = colbest[0][tx];
+        for (int y = 1; y < 8; y++) k = kmax(k, colbest[y][tx]);
+        if (k && b < n) atomicMax(&rowbest[b], k);
+    }
+}
+
+// Candidate keys: one per row whose best partner improves, deduplicated when
+// two rows pick each other.  Sort key: (0x7fffffff - delta) << 32 | lo << 16 | hi
+// -> ascending order = delta desc, lo asc, hi asc.  Rows without a candidate
+// get ~0.
+__global__ void k_candidates(const unsigned long long* __restrict__ rowbest, int n,
+                             unsigned long long* __restrict__ keys, int* __restrict__ ncand,
+                             int* __restrict__ best_delta) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n) return;
+    const unsigned long long k = rowbest[a];
+    unsigned long long out = ~0ull;
+    if (k) {
+        const int d = (int)((unsigned)(k >> 32) - 0x80000000u);
+        const int b = (int)(~(unsigned)(k & 0xffffffffu));
+        if (d > 0) {
+            atomicMax(best_delta, d);
+            const unsigned long long kb = rowbest[b];
+            const int bb = (int)(~(unsigned)(kb & 0xffffffffu));
+            const bool mutual = (kb != 0) && (bb == a);
+            if (!mutual || a < b) {
+                const int lo = a < b ? a : b, hi = a < b ? b : a;
+                out = ((unsigned long long)(0x7fffffffu - (unsigned)d) << 32) |
+                      ((unsigned long long)lo << 16) | (unsigned long long)hi;
+                atomicAdd(ncand, 1);
+            }
+        }
+    }
+    keys[a] = out;
+}
+
+// ---------------------------------------------------------------------------
+// Exact swap delta of (a,b) on the current matching, one element of the four
+// edge lists per thread of the group, as calculate_swap_delta computes it
+// (src/graph-alignment-optimized.c:321-408), plus the exact self-loop terms.
+template <bool W16>
+__device__ __forceinline__ int swap_delta_part(const DevView<W16>& g, int a, int b, int t, int nt) {
+    typedef Ent<W16> EN;
+    const int pa = g.p[a], pb = g.p[b];
+    int d = 0;
+    const int la0 = g.off1o[a], la = g.off1o[a + 1] - la0;
+    const int ia0 = g.off1i[a], ia = g.off1i[a + 1] - ia0;
+    const int lb0 = g.off1o[b], lb = g.off1o[b + 1] - lb0;
+    const int ib0 = g.off1i[b], ib = g.off1i[b + 1] - ib0;
+    const int tot = la + ia + lb + ib;
+    for (int k = t; k < tot; k += nt) {
+        int q = k;
+        if (q < la) {  // out-edge a->v
+            const typename EN::T e = g.ent1o[la0 + q];
+            const int v = EN::id(e), w = EN::w(e);
+            if (v == b) d += imin(w, g.w2(pb, pa)) - imin(w, g.w2(pa, pb));
+            else { const int pv = g.p[v]; d += imin(w, g.w2(pb, pv)) - imin(w, g.w2(pa, pv)); }
+            continue;
+        }
+        q -= la;
+        if (q < ia) {  // in-edge u->a
+            const typename EN::T e = g.ent1i[ia0 + q];
+            const int u = EN::id(e), w = EN::w(e);
+            if (u != b) { const int pu = g.p[u]; d += imin(w, g.w2(pu, pb)) - imin(w, g.w2(pu, pa)); }
+            continue;  // the edge b->a is counted once, from b's out-list
+        }
+        q -= ia;
+        if (q < lb) {  // out-edge b->v
+            const typename EN::T e = g.ent1o[lb0 + q];
+            const int v = EN::id(e), w = EN::w(e);
+            if (v == a) d += imin(w, g.w2(pa, pb)) - imin(w, g.w2(pb, pa));
+            else { const int pv = g.p[v]; d += imin(w, g.w2(pa, pv)) - imin(w, g.w2(pb, pv)); }
+            continue;
+        }
+        q -= lb;
+        {  // in-edge u->b
+            const typename EN::T e = g.ent1i[ib0 + q];
+            const int u = EN::id(e), w = EN::w(e);
+            if (u != a) { const int pu = g.p[u]; d += imin(w, g.w2(pu, pa)) - imin(w, g.w2(pu, pb)); }
+        }
+    }
+    if (t == 0) {
+        for (int q = g.offs[a]; q < g.offs[a + 1]; q++)
+            d += imin(g.selfw[q], g.w2(pb, pb)) - imin(g.selfw[q], g.w2(pa, pa));
+        for (int q = g.offs[b]; q < g.offs[b + 1]; q++)
+            d += imin(g.selfw[q], g.w2(pa, pa)) - imin(g.selfw[q], g.w2(pb, pb));
+    }
+    return d;
+}
+
+// One warp per requested pair.
+template <bool W16>
+__global__ void k_pair_deltas(DevView<W16> g, const int* __restrict__ pa, const int* __restrict__ pb,
+                              long long k, int* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (; w < k; w += nw) {
+        int d = swap_delta_part<W16>(g, pa[w], pb[w], lane, 32);
+        for (int o = 16; o; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+        if (lane == 0) out[w] = d;
+    }
+}
+
+// Alignment score (src/graph-alignment-optimized.c:292-307): one warp per row.
+template <bool W16>
+__global__ void k_score(DevView<W16> g, unsigned long long* __restrict__ out) {
+    typedef Ent<W16> EN;
+    const int lane = threadIdx.x & 31;
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    long long s = 0;
+    for (int a = warp; a < g.n; a += nwarps) {
+        const int pa = g.p[a];
+        for (int i = g.off1o[a] + lane; i < g.off1o[a + 1]; i += 32) {
+            const typename EN::T e = g.ent1o[i];
+            s += imin(EN::w(e), g.w2(pa, g.p[EN::id(e)]));
+        }
+        if (lane == 0)
+            for (int q = g.offs[a]; q < g.offs[a + 1]; q++) s += imin(g.selfw[q], g.w2(pa, pa));
+    }
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0 && s) atomicAdd(out, (unsigned long long)s);
+}
+
+// ---------------------------------------------------------------------------
+// Sequential commit of sorted candidates (one CTA).
+//   used[x]  : x already moved in this sweep
+//   taint[x] : x is a G1 neighbour of a moved vertex, so its cached delta may
+//              be stale and must be re-evaluated before committing.
+// A candidate whose endpoints are untainted keeps its sweep delta exactly,
+// because a swap delta depends only on p at the two endpoints and at their
+// G1 neighbours.
+struct CommitStats {
+    long long total_delta;
+    int scanned, verified, committed, pad;
+};
+
+template <bool W16>
+__global__ void __launch_bounds__(1024)
+k_commit(DevView<W16> g, const unsigned long long* __restrict__ keys, int nkeys,
+         int max_scan, int max_verify, CommitStats* __restrict__ st, int* __restrict__ moves) {
+    typedef Ent<W16> EN;
+    extern __shared__ unsigned char flags[];  // used[n] then taint[n]
+    unsigned char* used = flags;
+    unsigned char* taint = flags + g.n;
+    __shared__ int red[32];
+    __shared__ int s_delta;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    for (int i = tid; i < 2 * g.n; i += blockDim.x) flags[i] = 0;
+    long long total = 0;
+    int scanned = 0, verified = 0, committed = 0;
+    __syncthreads();
+    const int lim = (max_scan > 0 && max_scan < nkeys) ? max_scan : nkeys;
+    for (int k = 0; k < lim; k++) {
+        const unsigned long long key = keys[k];
+        if (key == ~0ull) break;
+        const int lo = (int)((key >> 16) & 0xffffu), hi = (int)(key & 0xffffu);
+        const int d0 = (int)(0x7fffffffu - (unsigned)(key >> 32));
+        scanned++;
+        if (used[lo] | used[hi]) continue;
+        int d = d0;
+        if (taint[lo] | taint[hi]) {
+            if (max_verify >= 0 && verified >= max_verify) continue;
+            verified++;
+            int part = swap_delta_part<W16>(g, lo, hi, tid, blockDim.x);
+            for (int o = 16; o; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+            if (lane == 0) red[wid] = part;
+            __syncthreads();
+            if (wid == 0) {
+                int v = lane < (blockDim.x >> 5) ? red[lane] : 0;
+                for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                if (lane == 0) s_delta = v;
+            }
+            __syncthreads();
+            d = s_delta;
+            __syncthreads();
+        }
+        if (d <= 0) continue;
+        if (tid == 0) {
+            const int flo = g.p[lo], fhi = g.p[hi];
+            g.p[lo] = fhi; g.p[hi] = flo;
+            if (fhi < g.n) g.pinv[fhi] = lo;
+            if (flo < g.n) g.pinv[flo] = hi;
+            used[lo] = 1; used[hi] = 1;
+            if (moves) { moves[3 * committed] = lo; moves[3 * committed + 1] = hi; moves[3 * committed + 2] = d; }
+        }
+        total += d;
+        committed++;
+        // taint the G1 neighbourhoods of both endpoints
+        const int l0 = g.off1o[lo], l1 = g.off1o[lo + 1] - l0;
+        const int i0 = g.off1i[lo], i1 = g.off1i[lo + 1] - i0;
+        const int m0 = g.off1o[hi], m1 = g.off1o[hi + 1] - m0;
+        const int j0 = g.off1i[hi], j1 = g.off1i[hi + 1] - j0;
+        const int tot = l1 + i1 + m1 + j1;
+        for (int q = tid; q < tot; q += blockDim.x) {
+            int r = q, x;
+            if (r < l1) x = EN::id(g.ent1o[l0 + r]);
+            else if ((r -= l1) < i1) x = EN::id(g.ent1i[i0 + r]);
+            else if ((r -= i1) < m1) x = EN::id(g.ent1o[m0 + r]);
+            else { r -= m1; x = EN::id(g.ent1i[j0 + r]); }
+            taint[x] = 1;
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        st->total_delta = total;
+        st->scanned = scanned;
+        st->verified = verified;
+        st->committed = committed;
+    }
+}
+
+}  // namespace bm

@@ -1,0 +1,298 @@
+/*
+ * bm.h -- C ABI of the B200 swap-delta engine for brain-match graph alignment.
+ *
+ * Problem: two directed, integer-weighted graphs G1 ("male", gm) and G2
+ * ("female", gf) on vertex ids 1..n, and a matching map[m] = f (G1 -> G2,
+ * 1-based, map[0] unused, 0 = unmatched).  The alignment score is
+ *
+ *     score(map) = sum over G1 edges (u,v,w):  min(w, w2(map[u], map[v]))
+ *
+ * (brain-match src/graph-alignment-optimized.c:292-307).  The engine computes
+ * the exact change of that score for swaps map[a] <-> map[b] and for 3-cycles,
+ * and hill-climbs by committing improving moves.
+ *
+ * Every function returns a bm_status (0 = OK, negative = error) and never
+ * calls exit().  The caller owns every host array it passes; arrays are copied
+ * in or out before the call returns.  The context owns all device memory.  One
+ * host thread per context; contexts are independent.
+ *
+ * Graph semantics follow the reference loaders
+ * (src/graph-alignment-optimized.c:183-204,635-679):
+ *   - G1 edges are summed per list entry, so duplicate G1 edges each count
+ *     (the reference keeps every copy in its edge lists);
+ *   - G2 is looked up as a dense matrix, so a repeated G2 edge keeps the LAST
+ *     weight given (the reference overwrites adj_matrix[from][to]);
+ *   - zero-weight edges contribute nothing and are dropped; negative weights
+ *     and ids outside 1..n are rejected with BM_E_INPUT.
+ * Deltas are mathematically exact.  They equal the reference's
+ * calculate_swap_delta whenever G1 has no self-loops and no repeated edge
+ * between the two swapped vertices (the reference is inexact there), and
+ * weights are <= 32767 (the reference stores weights in `short`).
+ */
+#ifndef BM_H
+#define BM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t bm_status;
+#define BM_OK          0
+#define BM_E_INPUT    -1   /* bad argument, malformed graph or mapping        */
+#define BM_E_CUDA     -2   /* a CUDA call failed (no device, launch error ...) */
+#define BM_E_OVERFLOW -3   /* a delta could exceed int32                       */
+#define BM_E_TIMEOUT  -4   /* a bounded device wait ran out                    */
+#define BM_E_NOMEM    -5   /* host or device allocation failed                 */
+#define BM_E_STATE    -6   /* call out of order (e.g. no mapping set)          */
+#define BM_E_IO       -7   /* file could not be opened / written               */
+
+/* Flags for bm_create. */
+#define BM_FLAG_FORCE_I32  0x1u  /* int32 entries even when 16-bit ones fit */
+
+typedef struct bm_ctx bm_ctx;
+
+/* Human-readable name of a status code (static string). */
+const char* bm_status_string(bm_status s);
+
+/* Text of the last error on this context ("" if none).  ctx may be NULL, in
+ * which case the last error of a failed bm_create on this thread is returned. */
+const char* bm_last_error(const bm_ctx* ctx);
+
+/*
+ * Build a context on the current CUDA device from two COO edge lists with
+ * 1-based vertex ids in 1..n.
+ * Replaces: load_graph_from_csv + new_graph/add_edge + the host->device copies
+ * of the dense matrices (src/graph-alignment-optimized.c:125-204,635-679;
+ * src/quick.cu:1047-1062).  Storage is chosen per input: 16-bit entries when
+ * n <= 65536 and min(max w1, max w2) <= 65535 (results stay exact), 32-bit
+ * otherwise or with BM_FLAG_FORCE_I32.
+ */
+bm_status bm_create(bm_ctx** out, int32_t n,
+                    int64_t e1, const int32_t* src1, const int32_t* dst1, const int32_t* w1,
+                    int64_t e2, const int32_t* src2, const int32_t* dst2, const int32_t* w2,
+                    uint32_t flags);
+
+void bm_destroy(bm_ctx* ctx);
+
+/* Information about a context. */
+typedef struct {
+    int32_t n;
+    int32_t entry_bits;      /* 16 or 32 */
+    int64_t e1, e2;          /* stored list entries (after drops/dedupe)   */
+    int64_t g1_self_loops;   /* G1 self-loop entries (handled exactly)     */
+    int64_t device_bytes;    /* device memory held by the context          */
+    int32_t device;          /* CUDA ordinal                               */
+    int32_t num_sms;
+} bm_info;
+bm_status bm_get_info(const bm_ctx* ctx, bm_info* info);
+
+/*
+ * Set / read the matching, map[1..n] in 1..n (0 = unmatched), an injective map.
+ * Mirrors the int mapping[NUM_NODES+1] of the reference
+ * (src/graph-alignment-optimized.c:428-475, src/quick.cu:1163-1166).
+ */
+bm_status bm_set_mapping(bm_ctx* ctx, const int32_t* map);
+bm_status bm_get_mapping(bm_ctx* ctx, int32_t* map);
+
+/*
+ * Alignment score of the current matching.
+ * Replaces calculate_alignment_score (src/graph-alignment-optimized.c:292-307).
+ */
+bm_status bm_score(bm_ctx* ctx, int64_t* score);
+
+/*
+ * Exact swap deltas for k given pairs (m1[i], m2[i]), 1-based, m1 != m2.
+ * Replaces calculate_swap_delta (src/graph-alignment-optimized.c:321-408).
+ */
+bm_status bm_pair_deltas(bm_ctx* ctx, int64_t k, const int32_t* m1, const int32_t* m2,
+                         int32_t* out);
+
+/*
+ * Exact deltas of all n(n-1)/2 unordered pairs in the reference's linear pair
+ * order (index 0 = (1,2), (1,3), ..., (1,n), (2,3), ...), written to the host
+ * array out.  Replaces calculateSwapDeltasKernel + its D2H copy
+ * (src/graph-re-alignment-gpu.cu:38-131,845-857; src/quick.cu:48-137).
+ */
+bm_status bm_all_deltas(bm_ctx* ctx, int32_t* out);
+
+/*
+ * Per-vertex profit row: out[b-1] = score that vertex a would contribute if it
+ * took map[b] with every other vertex fixed (b = 1..n); out[a-1] is a's current
+ * contribution.  Diagnostic view of the matrix the sweep is built on.
+ */
+bm_status bm_profit_row(bm_ctx* ctx, int32_t a, int32_t* out);
+
+/* ---- Pairwise hill-climbing sweep (full all-pairs evaluation + commit) ---- */
+typedef struct {
+    int32_t max_candidates;  /* sorted candidates scanned per sweep (<=0: all)   */
+    int32_t max_verify;      /* re-verifications of tainted candidates (<0: all) */
+    int32_t reserved[6];
+} bm_sweep_opts;
+
+typedef struct {
+    int64_t score_before;
+    int64_t score_after;
+    int64_t deltas_evaluated;   /* n(n-1)/2 per sweep                   */
+    int32_t candidates;         /* rows whose best swap is improving     */
+    int32_t scanned;            /* candidates looked at by the commit    */
+    int32_t verified;           /* tainted candidates re-evaluated       */
+    int32_t committed;          /* swaps applied                         */
+    int32_t best_delta;         /* largest delta of the sweep            */
+    int32_t reserved;
+    /* device time (CUDA events on the context's stream), milliseconds:      */
+    float   ms_profit;          /* profit-row kernel alone                */
+    float   ms_combine;         /* pair combine + per-row best            */
+    float   ms_commit;          /* candidate sort + sequential commit     */
+    float   ms_total;           /* whole sweep                            */
+    float   ms_prep;            /* relabelling + row scheduling           */
+    int32_t pad;
+    int64_t min_terms;          /* nonzero min terms scattered            */
+} bm_sweep_stats;
+
+/*
+ * One sweep: evaluate every pair, take each vertex's best partner, sort the
+ * improving ones by (delta desc, lower id asc, higher id asc), then in that
+ * order commit each pair whose vertices are still untouched and whose delta,
+ * re-evaluated on the updated matching, is still > 0.
+ * Replaces the sweep + host argmax + commit of src/graph-re-alignment-gpu.cu:
+ * 845-891 and the best-per-row loop of src/alignment-omp.c:601-658.
+ */
+bm_status bm_sweep(bm_ctx* ctx, const bm_sweep_opts* opts, bm_sweep_stats* stats);
+
+/*
+ * Sweeps until no improving swap remains or max_sweeps is reached.
+ * per_sweep (may be NULL) receives one record per sweep.
+ */
+bm_status bm_hillclimb(bm_ctx* ctx, int32_t max_sweeps, const bm_sweep_opts* opts,
+                       bm_sweep_stats* per_sweep, int32_t* sweeps_done);
+
+/*
+ * The reference's sequential first-improvement order
+ * (src/graph-alignment-optimized.c:515-577): for m1 = 1..n, for m2 = 1..n,
+ * m2 != m1, commit the swap if its delta on the current matching is > 0.
+ * Runs up to max_passes full passes, stopping after a pass with no commit
+ * (the reference loops forever).  Commits and passes are reported.
+ */
+bm_status bm_first_improvement(bm_ctx* ctx, int32_t max_passes, int64_t* commits,
+                               int32_t* passes_done);
+
+/*
+ * Device timer on the context's stream: record event `slot` (0..7) now, and
+ * read the elapsed milliseconds between two recorded slots (synchronizes).
+ * Lets a caller time a run of calls on the device, e.g. K sweeps.
+ */
+bm_status bm_timer_mark(bm_ctx* ctx, int32_t slot);
+bm_status bm_timer_elapsed(bm_ctx* ctx, int32_t start_slot, int32_t end_slot, float* ms);
+
+/* ---- 3-cycles ---- */
+
+/*
+ * Exact deltas of the two cyclic rotations of each triple (a[i],b[i],c[i]),
+ * distinct 1-based ids:  out[2i]   = delta of (map[a],map[b],map[c]) <- (f2,f3,f1)
+ *                        out[2i+1] = delta of (map[a],map[b],map[c]) <- (f3,f1,f2)
+ * i.e. permutations 3 and 4 of calculateThreeNodeSwapKernel
+ * (src/triple.cu:85-92) as applied by apply_permutation (src/triple.cu:903-934).
+ */
+bm_status bm_triple_deltas(bm_ctx* ctx, int64_t k, const int32_t* a, const int32_t* b,
+                           const int32_t* c, int32_t* out);
+
+typedef struct {
+    int32_t partners;        /* 2-hop samples per vertex (256)            */
+    int32_t max_candidates;  /* sorted candidates scanned (<=0: all)      */
+    int32_t max_verify;      /* re-verifications (<0: all)                */
+    int32_t reserved0;
+    uint64_t seed;           /* round seed for the 2-hop sampler          */
+    int32_t reserved[4];
+} bm_triple_opts;
+
+typedef struct {
+    int64_t score_before, score_after;
+    int64_t triples;            /* valid sampled triples               */
+    int64_t rotations;          /* 2 per triple                        */
+    int32_t candidates, scanned, verified, committed;
+    int32_t best_delta, reserved;
+    float   ms_sample, ms_eval, ms_commit, ms_total;
+} bm_triple_stats;
+
+/*
+ * One 3-cycle round: sample `partners` 2-hop paths (a -> b -> c, undirected
+ * G1 neighbourhoods) per vertex a, evaluate both rotations of each triple
+ * exactly, and commit the best vertex-disjoint improving set under the same
+ * re-verification rule as bm_sweep.  Replaces the batch loop of
+ * src/triple.cu:1074-1157 (which visits only a few batches per pass).
+ */
+bm_status bm_triple_round(bm_ctx* ctx, const bm_triple_opts* opts, bm_triple_stats* stats);
+
+/* ---- Host utilities: file formats and the synthetic generator ---- */
+
+/* Free memory returned by the readers below. */
+void bm_free(void* p);
+
+/*
+ * Graph CSV: one header line, then "from,to,weight" integers.  Malformed lines
+ * are skipped with a message on stderr, as load_graph_from_csv does
+ * (src/graph-alignment-optimized.c:635-679).  Arrays are malloc'd; release
+ * them with bm_free.
+ */
+bm_status bm_read_graph_csv(const char* path, int64_t* e, int32_t** src, int32_t** dst,
+                            int32_t** w, int32_t* max_id);
+
+/*
+ * Matching CSV: one header line, then "m<id>,f<id>" or "<id>,<id>" lines, as
+ * load_benchmark_mapping reads them (src/graph-alignment-optimized.c:428-475).
+ * map must hold n+1 entries; it is zeroed first.  Ids outside 1..n are
+ * rejected.  *count receives the number of lines read.
+ */
+bm_status bm_read_mapping_csv(const char* path, int32_t n, int32_t* map, int32_t* count);
+
+/*
+ * Writes "Male Node ID,Female Node ID" then "m%d,f%d" for every map[i] != 0,
+ * exactly as write_mapping (src/graph-alignment-optimized.c:410-425).
+ */
+bm_status bm_write_mapping_csv(const char* path, int32_t n, const int32_t* map);
+
+/*
+ * Numeric matching format of refine-matching-hillclimb: header
+ * "Male ID,Female ID" then "%d,%d" (src/refine-matching-hillclimb.c:454-503).
+ */
+bm_status bm_write_mapping_csv_numeric(const char* path, int32_t n, const int32_t* map);
+
+/* Synthetic graph-pair generator (seeded, deterministic). */
+typedef struct {
+    int32_t n;             /* vertices                                           */
+    int32_t wmax;          /* weight cap                                         */
+    int64_t e;             /* G1 edges                                           */
+    uint64_t seed;
+    double  alpha;         /* out-degree power-law exponent (2.1)                */
+    double  geom_p;        /* weight = 1 + Geometric(geom_p) failures (0.35)     */
+    double  tail_prob;     /* probability of a heavy-tail weight (0 or 1e-3)     */
+    double  tail_alpha;    /* heavy tail: floor(tail_scale * Pareto(tail_alpha)) */
+    double  tail_scale;
+    double  del_frac;      /* G2: fraction of relabelled G1 edges deleted (0.1)  */
+    double  add_frac;      /* G2: random edges added, as a fraction of e (0.1)   */
+    int32_t jitter;        /* G2: every weight += uniform{-jitter..jitter}, >= 1 */
+    int32_t reserved;
+} bm_gen_params;
+
+/* Fills p with the defaults of the N=1,000 / 20,000-edge workload. */
+void bm_gen_defaults(bm_gen_params* p);
+
+/*
+ * Generates G1 (exactly e edges, no self-loops, no duplicates, sorted by
+ * (src,dst)), G2 = G1 relabelled by a random permutation with edges deleted,
+ * added and jittered (sorted), and a uniform random initial matching.
+ * Capacities: src1/dst1/w1 hold e entries, src2/dst2/w2 hold
+ * e + ceil(add_frac*e) entries; pi and map0 hold n+1 entries (1-based; pi is
+ * the hidden G1 -> G2 relabelling).  *e2 receives G2's edge count.
+ */
+bm_status bm_generate(const bm_gen_params* prm,
+                      int32_t* src1, int32_t* dst1, int32_t* w1,
+                      int64_t* e2, int32_t* src2, int32_t* dst2, int32_t* w2,
+                      int32_t* pi, int32_t* map0);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BM_H */

@@ -1,0 +1,204 @@
+"""ctypes binding of the CPU oracle -- TEST INFRASTRUCTURE ONLY.
+
+Loads oracle/_ref/liboracle.so (the C restatement, bm_oracle.c) and, when they
+were built, the reference's own code compiled in place:
+oracle/_ref/librefgao.so (src/graph-alignment-optimized.c) and
+oracle/_ref/librefperm.so (src/permutation.c).  Only tests/, smoke() and
+bench.py's CPU-baseline leg import this module, as the checker.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(_HERE, "_ref")
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _load(name):
+    path = os.path.join(REF_DIR, name)
+    return C.CDLL(path) if os.path.exists(path) else None
+
+
+vp, i32, i64, u64 = C.c_void_p, C.c_int32, C.c_int64, C.c_uint64
+_orc = None
+
+
+def orc_lib():
+    global _orc
+    if _orc is None:
+        L = C.CDLL(os.path.join(REF_DIR, "liboracle.so"))
+        L.orc_create.restype = vp
+        L.orc_create.argtypes = [i32, i64, vp, vp, vp, i64, vp, vp, vp]
+        L.orc_free.argtypes = [vp]
+        L.orc_free.restype = None
+        L.orc_score.restype = i64
+        L.orc_score.argtypes = [vp, vp]
+        L.orc_swap_delta.argtypes = [vp, vp, i32, i32]
+        L.orc_all_deltas.argtypes = [vp, vp, vp]
+        L.orc_all_deltas.restype = None
+        L.orc_sweep.argtypes = [vp, vp, i32, i32, vp, vp]
+        L.orc_first_improvement.restype = i64
+        L.orc_first_improvement.argtypes = [vp, vp, i32, C.POINTER(i32), C.POINTER(i64)]
+        L.orc_local_score.restype = i64
+        L.orc_local_score.argtypes = [vp, vp, vp, i32]
+        L.orc_triple_delta.argtypes = [vp, vp, i32, i32, i32, i32]
+        L.orc_sample_triple.argtypes = [vp, u64, i32, i32, C.POINTER(i32), C.POINTER(i32)]
+        L.orc_triple_round.argtypes = [vp, vp, i32, u64, i32, i32, vp]
+        _orc = L
+    return _orc
+
+
+class Oracle:
+    """The C restatement (bm_oracle.c) over one graph pair (1-based ids)."""
+
+    def __init__(self, n, src1, dst1, w1, src2, dst2, w2):
+        self._keep = [np.ascontiguousarray(x, np.int32) for x in (src1, dst1, w1, src2, dst2, w2)]
+        a = self._keep
+        self.n = int(n)
+        self.h = orc_lib().orc_create(self.n, len(a[0]), _p(a[0]), _p(a[1]), _p(a[2]),
+                                      len(a[3]), _p(a[3]), _p(a[4]), _p(a[5]))
+
+    @classmethod
+    def from_pair(cls, g):
+        return cls(g["n"], g["src1"], g["dst1"], g["w1"], g["src2"], g["dst2"], g["w2"])
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            orc_lib().orc_free(self.h)
+            self.h = None
+
+    def score(self, m):
+        m = np.ascontiguousarray(m, np.int32)
+        return orc_lib().orc_score(self.h, _p(m))
+
+    def swap_delta(self, m, a, b):
+        m = np.ascontiguousarray(m, np.int32)
+        return orc_lib().orc_swap_delta(self.h, _p(m), int(a), int(b))
+
+    def all_deltas(self, m):
+        m = np.ascontiguousarray(m, np.int32)
+        out = np.zeros(self.n * (self.n - 1) // 2, np.int32)
+        orc_lib().orc_all_deltas(self.h, _p(m), _p(out))
+        return out
+
+    def sweep(self, m, max_candidates=0, max_verify=-1, want_moves=False):
+        """Runs one sweep IN PLACE on m (int32 array); returns stats dict."""
+        st = np.zeros(8, np.int64)
+        mv = np.zeros(3 * (self.n + 1), np.int32) if want_moves else None
+        c = orc_lib().orc_sweep(self.h, _p(m), max_candidates, max_verify, _p(st),
+                                _p(mv) if mv is not None else None)
+        d = dict(total_delta=int(st[0]), candidates=int(st[1]), scanned=int(st[2]), verified=int(st[3]),
+                 committed=int(st[4]), best_delta=int(st[5]), deltas=int(st[6]))
+        if want_moves:
+            d["moves"] = mv[:3 * c].reshape(-1, 3)
+        return d
+
+    def first_improvement(self, m, max_passes):
+        p, ds = i32(), i64()
+        c = orc_lib().orc_first_improvement(self.h, _p(m), max_passes, C.byref(p), C.byref(ds))
+        return c, p.value, ds.value
+
+    def triple_delta(self, m, a, b, c, rot):
+        m = np.ascontiguousarray(m, np.int32)
+        return orc_lib().orc_triple_delta(self.h, _p(m), a, b, c, rot)
+
+    def local_score(self, m, vs):
+        m = np.ascontiguousarray(m, np.int32)
+        vs = np.ascontiguousarray(vs, np.int32)
+        return orc_lib().orc_local_score(self.h, _p(m), _p(vs), len(vs))
+
+    def sample_triple(self, seed, a, j):
+        b, c = i32(), i32()
+        ok = orc_lib().orc_sample_triple(self.h, seed, a, j, C.byref(b), C.byref(c))
+        return (b.value, c.value) if ok else None
+
+    def triple_round(self, m, partners=256, seed=0, max_candidates=0, max_verify=-1):
+        st = np.zeros(8, np.int64)
+        orc_lib().orc_triple_round(self.h, _p(m), partners, seed, max_candidates, max_verify, _p(st))
+        return dict(total_delta=int(st[0]), candidates=int(st[1]), scanned=int(st[2]), verified=int(st[3]),
+                    committed=int(st[4]), best_delta=int(st[5]), triples=int(st[6]))
+
+
+class RefGAO:
+    """The reference's src/graph-alignment-optimized.c, compiled in place."""
+
+    def __init__(self, lib=None):
+        L = lib or _load("librefgao.so")
+        if L is None:
+            raise OSError("oracle/_ref/librefgao.so not built")
+        L.refgao_graph_new.restype = vp
+        L.refgao_graph_add_many.argtypes = [vp, i64, vp, vp, vp]
+        L.refgao_graph_add_many.restype = None
+        L.refgao_graph_free.argtypes = [vp]
+        L.refgao_graph_free.restype = None
+        L.refgao_score.argtypes = [vp, vp, vp]
+        L.refgao_swap_delta.argtypes = [vp, vp, vp, i32, i32]
+        L.refgao_pair_deltas.argtypes = [vp, vp, vp, i64, vp, vp, vp]
+        L.refgao_pair_deltas.restype = None
+        L.refgao_rows_omp.restype = i64
+        L.refgao_rows_omp.argtypes = [vp, vp, vp, vp, i32, i32, C.POINTER(i64), C.POINTER(i32)]
+        self.L = L
+        self.NUM_NODES = L.refgao_num_nodes()
+
+    def graph(self, s, d, w):
+        g = self.L.refgao_graph_new()
+        a = [np.ascontiguousarray(x, np.int32) for x in (s, d, w)]
+        self.L.refgao_graph_add_many(g, len(a[0]), _p(a[0]), _p(a[1]), _p(a[2]))
+        return g
+
+    def pad(self, m):
+        """The reference indexes mappings up to NUM_NODES."""
+        out = np.zeros(max(self.NUM_NODES, len(m) - 1) + 1, np.int32)
+        out[:len(m)] = m
+        return out
+
+    def score(self, gm, gf, m):
+        mp = self.pad(m)
+        return self.L.refgao_score(gm, gf, _p(mp))
+
+    def pair_deltas(self, gm, gf, m, a, b):
+        mp = self.pad(m)
+        a = np.ascontiguousarray(a, np.int32)
+        b = np.ascontiguousarray(b, np.int32)
+        out = np.zeros(len(a), np.int32)
+        self.L.refgao_pair_deltas(gm, gf, _p(mp), len(a), _p(a), _p(b), _p(out))
+        return out
+
+    def rows_omp(self, gm, gf, m, rows, n):
+        mp = self.pad(m)
+        rows = np.ascontiguousarray(rows, np.int32)
+        cs, nt = i64(), i32()
+        cnt = self.L.refgao_rows_omp(gm, gf, _p(mp), _p(rows), len(rows), n, C.byref(cs), C.byref(nt))
+        return cnt, cs.value, nt.value
+
+
+class RefPerm:
+    """The reference's src/permutation.c, compiled in place."""
+
+    def __init__(self):
+        L = _load("librefperm.so")
+        if L is None:
+            raise OSError("oracle/_ref/librefperm.so not built")
+        L.refperm_graph_new.restype = vp
+        L.refperm_graph_add_many.argtypes = [vp, i64, vp, vp, vp]
+        L.refperm_graph_add_many.restype = None
+        L.refperm_local_score.argtypes = [vp, vp, vp, vp, i32]
+        L.refperm_score.argtypes = [vp, vp, vp]
+        self.L = L
+
+    def graph(self, s, d, w):
+        g = self.L.refperm_graph_new()
+        a = [np.ascontiguousarray(x, np.int32) for x in (s, d, w)]
+        self.L.refperm_graph_add_many(g, len(a[0]), _p(a[0]), _p(a[1]), _p(a[2]))
+        return g
+
+    def local_score(self, gm, gf, m, vs):
+        mp = np.zeros(max(18524, len(m) - 1) + 1, np.int32)
+        mp[:len(m)] = m
+        vs = np.ascontiguousarray(vs, np.int32)
+        return self.L.refperm_local_score(gm, gf, _p(mp), _p(vs), len(vs))

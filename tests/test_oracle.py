@@ -1,0 +1,81 @@
+"""CPU tests: the oracle pinned against the reference (golden fixtures made by
+running the reference's own code, and the compiled reference when present)."""
+import numpy as np
+import pytest
+
+import oracle
+from conftest import GOLDEN_CASES, load_golden
+
+
+def _pair(z):
+    return oracle.Oracle(int(z["n"]), z["src1"], z["dst1"], z["w1"], z["src2"], z["dst2"], z["w2"])
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_oracle_matches_reference_golden(name):
+    z = load_golden(name)
+    O = _pair(z)
+    m = z["map0"]
+    assert O.score(m) == int(z["ref_score"])
+    d = O.all_deltas(m)
+    n = int(z["n"])
+    a, b = np.triu_indices(n, 1)
+    exact = d[z["pair_idx"]]
+    # every delta equals the reference's score difference (exactness)
+    assert np.array_equal(exact.astype(np.int64), z["ref_score_diff"])
+    if name == "g1_self_loops_n50":
+        # the reference delta double-counts G1 self-loops; the oracle is exact
+        loops = set(int(s) for s, t in zip(z["src1"], z["dst1"]) if s == t)
+        touched = np.array([(x + 1) in loops or (y + 1) in loops for x, y in zip(a, b)])
+        assert np.array_equal(d[~touched], z["ref_deltas"][~touched])
+        assert (d[touched] != z["ref_deltas"][touched]).any()
+    else:
+        assert np.array_equal(d, z["ref_deltas"])
+    # 3-cycles: local-score differences of the reference's calculate_permutation_delta
+    for t, (x, y, w) in enumerate(z["triples"]):
+        for rot in range(2):
+            ref = int(z["ref_local"][t, 1 + rot] - z["ref_local"][t, 0])
+            assert O.triple_delta(m, int(x), int(y), int(w), rot) == ref
+
+
+def test_oracle_matches_compiled_reference_cfg0(cfg0):
+    try:
+        R = oracle.RefGAO()
+    except OSError:
+        pytest.skip("reference not compiled on this machine")
+    g = cfg0
+    O = oracle.Oracle.from_pair(g)
+    gm = R.graph(g["src1"], g["dst1"], g["w1"])
+    gf = R.graph(g["src2"], g["dst2"], g["w2"])
+    m = g["map0"]
+    assert O.score(m) == R.score(gm, gf, m)
+    n = g["n"]
+    a, b = np.triu_indices(n, 1)
+    assert np.array_equal(O.all_deltas(m), R.pair_deltas(gm, gf, m, a + 1, b + 1))
+
+
+def test_oracle_sweep_rule_properties(cfg0):
+    g = cfg0
+    O = oracle.Oracle.from_pair(g)
+    m = g["map0"].copy()
+    s = O.score(m)
+    for _ in range(3):
+        st = O.sweep(m, want_moves=True)
+        s2 = O.score(m)
+        assert s2 == s + st["total_delta"]
+        assert st["total_delta"] == int(st["moves"][:, 2].sum())
+        assert (st["moves"][:, 2] > 0).all()
+        assert sorted(m[1:]) == list(range(1, g["n"] + 1))
+        s = s2
+
+
+def test_oracle_first_improvement_terminates():
+    z = load_golden("small_n40")
+    O = _pair(z)
+    m = z["map0"].copy()
+    s0 = O.score(m)
+    c, passes, dsum = O.first_improvement(m, 1000)
+    assert O.score(m) == s0 + dsum
+    assert c > 0
+    # at the fixed point no swap improves
+    assert (O.all_deltas(m) <= 0).all()
