@@ -184,9 +184,10 @@ def test_bad_mapping_and_call_order_errors():
 def test_large_weights_use_int32_path():
     rng = np.random.default_rng(3)
     n = 200
+    # both sides above 65535 (so 16-bit entries cannot be exact), loads below the overflow guard
     z = dict(n=n, src1=rng.integers(1, n + 1, 3000), dst1=rng.integers(1, n + 1, 3000),
-             w1=rng.integers(1, 10**8, 3000), src2=rng.integers(1, n + 1, 3000),
-             dst2=rng.integers(1, n + 1, 3000), w2=rng.integers(1, 10**8, 3000))
+             w1=rng.integers(65536, 10**6, 3000), src2=rng.integers(1, n + 1, 3000),
+             dst2=rng.integers(1, n + 1, 3000), w2=rng.integers(65536, 10**6, 3000))
     m = np.zeros(n + 1, np.int32); m[1:] = rng.permutation(n) + 1
     O = _oracle(z)
     with _engine(z) as E:
