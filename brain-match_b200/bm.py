@@ -15,6 +15,7 @@ LIB_PATH = os.path.join(_HERE, "lib", "libbm.so")
 BM_OK, BM_E_INPUT, BM_E_CUDA, BM_E_OVERFLOW, BM_E_TIMEOUT, BM_E_NOMEM, BM_E_STATE, BM_E_IO = (
     0, -1, -2, -3, -4, -5, -6, -7)
 BM_FLAG_FORCE_I32 = 1
+BM_STATIC_MAX_PAIRS = 65536
 
 
 class GenParams(C.Structure):
@@ -81,6 +82,7 @@ def lib():
         L.bm_score.argtypes = [vp, C.POINTER(i64)]
         L.bm_pair_deltas.argtypes = [vp, i64, vp, vp, vp]
         L.bm_profit_row.argtypes = [vp, i32, vp]
+        L.bm_pair_deltas_static.argtypes = [vp, i64, vp, vp, vp]
         L.bm_sweep.argtypes = [vp, C.POINTER(SweepOpts), C.POINTER(SweepStats)]
         L.bm_hillclimb.argtypes = [vp, i32, C.POINTER(SweepOpts), vp, C.POINTER(i32)]
         L.bm_first_improvement.argtypes = [vp, i32, C.POINTER(i64), C.POINTER(i32)]
@@ -199,6 +201,14 @@ class Engine:
         m2 = np.ascontiguousarray(m2, np.int32)
         out = np.zeros(len(m1), np.int32)
         _check(lib().bm_pair_deltas(self.h, len(m1), _p(m1), _p(m2), _p(out)), self.h)
+        return out
+
+    def pair_deltas_static(self, m1, m2):
+        """bm_pair_deltas_static: same deltas, staged in the library's fixed array."""
+        m1 = np.ascontiguousarray(m1, np.int32)
+        m2 = np.ascontiguousarray(m2, np.int32)
+        out = np.zeros(len(m1), np.int32)
+        _check(lib().bm_pair_deltas_static(self.h, len(m1), _p(m1), _p(m2), _p(out)), self.h)
         return out
 
     def all_deltas(self):

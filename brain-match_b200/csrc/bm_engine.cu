@@ -10,6 +10,7 @@
 #include <vector>
 #include <algorithm>
 #include <utility>
+#include <mutex>
 #include <cuda_runtime.h>
 #include <cub/device/device_radix_sort.cuh>
 #include "bm.h"
@@ -780,4 +781,92 @@ extern "C" bm_status bm_triple_round(bm_ctx* ctx, const bm_triple_opts* opts, bm
     if (!ctx || !opts) return BM_E_INPUT;
     if (!ctx->mapped) { set_err(ctx, "bm_triple_round: no mapping set"); return BM_E_STATE; }
     return ctx->w16 ? triple_round_impl<true>(ctx, opts, stats) : triple_round_impl<false>(ctx, opts, stats);
+}
+
+// ---------------------------------------------------------------------------
+// bm_pair_deltas_static: staging in a fixed library array instead of memory
+// the context allocates.  Layout: [0,K) first vertices, [K,2K) second
+// vertices (both 1-based, as the caller passed them), [2K,3K) deltas, with
+// K = BM_STATIC_MAX_PAIRS.  The host only ever uses the array's device address
+// obtained from cudaGetSymbolAddress; the symbol itself is a host-side stand-in.
+static __device__ __align__(256) int g_static_pairs[3 * BM_STATIC_MAX_PAIRS];
+
+namespace {
+constexpr int kStaticMaxDevices = 64;
+std::mutex g_static_mu;
+int* g_static_addr[kStaticMaxDevices] = {};
+}  // namespace
+
+// One warp per pair; ids arrive 1-based straight from the caller's arrays.
+template <bool W16>
+__global__ void k_pair_deltas_static(DevView<W16> g, const int* __restrict__ m1,
+                                     const int* __restrict__ m2, long long k, int* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (; w < k; w += nw) {
+        int d = swap_delta_part<W16>(g, m1[w] - 1, m2[w] - 1, lane, 32);
+        for (int o = 16; o; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+        if (lane == 0) out[w] = d;
+    }
+}
+
+// Device address of g_static_pairs on the context's device, looked up once per
+// device with that device current.
+static bm_status static_pairs_addr(bm_ctx* ctx, int** out) {
+    if (ctx->dev < 0 || ctx->dev >= kStaticMaxDevices) {
+        set_err(ctx, "bm_pair_deltas_static: device %d outside 0..%d", ctx->dev, kStaticMaxDevices - 1);
+        return BM_E_INPUT;
+    }
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (!g_static_addr[ctx->dev]) {
+        int cur = -1;
+        CK(cudaGetDevice(&cur));
+        if (cur != ctx->dev) CK(cudaSetDevice(ctx->dev));
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_static_pairs);
+        if (cur != ctx->dev) CK(cudaSetDevice(cur));
+        if (e != cudaSuccess) {
+            set_err(ctx, "bm_pair_deltas_static: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+            return BM_E_CUDA;
+        }
+        g_static_addr[ctx->dev] = static_cast<int*>(p);
+    }
+    *out = g_static_addr[ctx->dev];
+    return BM_OK;
+}
+
+extern "C" bm_status bm_pair_deltas_static(bm_ctx* ctx, int64_t k, const int32_t* m1, const int32_t* m2,
+                                           int32_t* out) {
+    if (!ctx) return BM_E_INPUT;
+    if (!ctx->mapped) { set_err(ctx, "bm_pair_deltas_static: no mapping set"); return BM_E_STATE; }
+    if (k < 0 || (k && (!m1 || !m2 || !out))) { set_err(ctx, "bm_pair_deltas_static: bad arguments"); return BM_E_INPUT; }
+    if (k > BM_STATIC_MAX_PAIRS) {
+        set_err(ctx, "bm_pair_deltas_static: k=%lld pairs exceeds the fixed staging size %d; split the call",
+                (long long)k, BM_STATIC_MAX_PAIRS);
+        return BM_E_INPUT;
+    }
+    if (k == 0) return BM_OK;
+    const int n = ctx->n;
+    for (int64_t i = 0; i < k; i++) {
+        if (m1[i] < 1 || m1[i] > n || m2[i] < 1 || m2[i] > n || m1[i] == m2[i]) {
+            set_err(ctx, "bm_pair_deltas_static: pair %lld = (%d,%d) invalid", (long long)i, m1[i], m2[i]);
+            return BM_E_INPUT;
+        }
+    }
+    int* base = nullptr;
+    bm_status s = static_pairs_addr(ctx, &base);
+    if (s) return s;
+    int* da = base;
+    int* db = base + BM_STATIC_MAX_PAIRS;
+    int* dout = base + 2 * BM_STATIC_MAX_PAIRS;
+    CK(cudaMemcpyAsync(da, m1, k * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(db, m2, k * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+    const long long blocks = std::min<long long>((k + 7) / 8, (long long)ctx->num_sms * 16);
+    if (ctx->w16) k_pair_deltas_static<true><<<(int)blocks, 256, 0, ctx->st>>>(view<true>(ctx), da, db, k, dout);
+    else k_pair_deltas_static<false><<<(int)blocks, 256, 0, ctx->st>>>(view<false>(ctx), da, db, k, dout);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, dout, k * sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return BM_OK;
 }

@@ -110,6 +110,41 @@ bm_status bm_pair_deltas(bm_ctx* ctx, int64_t k, const int32_t* m1, const int32_
                          int32_t* out);
 
 /*
+ * bm_pair_deltas_static -- the same deltas as bm_pair_deltas for up to
+ * BM_STATIC_MAX_PAIRS pairs, without allocating any memory.
+ * No counterpart in the reference.
+ *
+ * bm_pair_deltas stages the pairs and their results in device memory that the
+ * context allocates with cudaMalloc the first time a call needs more room.
+ * Some callers cannot let that happen:
+ *   - a process whose GPU memory is already handed out to another allocator
+ *     (a framework's caching allocator, a fixed memory pool), where a new
+ *     cudaMalloc fails or pushes the pool out of memory mid-search;
+ *   - a loop that scores a few candidate swaps between other GPU work, where
+ *     cudaMalloc/cudaFree can synchronize the whole device and stall the
+ *     other streams.
+ * This entry point stages through one fixed array compiled into the library
+ * (a static __device__ array of 3 * BM_STATIC_MAX_PAIRS int32, 768 KiB).  Every
+ * GPU that loads the library holds that array until the process exits.
+ *
+ * Limits and sharing:
+ *   - k > BM_STATIC_MAX_PAIRS is rejected with BM_E_INPUT; split the work.
+ *   - The first call on a device looks up the array's device address
+ *     (cudaGetSymbolAddress, with that device current) and keeps it; make
+ *     that first call before capturing any CUDA stream.
+ *   - All calls in the process share the one array, which keeps the last
+ *     call's contents.  Nothing in it has to start at zero: each call writes
+ *     every result it copies back.  Calls that overlap on the GPU (two
+ *     contexts, or two host threads, at the same time on one device) race on
+ *     the array; serialize them.  Each call waits for its own work before it
+ *     returns.
+ * Arguments and errors are those of bm_pair_deltas.
+ */
+#define BM_STATIC_MAX_PAIRS 65536
+bm_status bm_pair_deltas_static(bm_ctx* ctx, int64_t k, const int32_t* m1, const int32_t* m2,
+                                int32_t* out);
+
+/*
  * Exact deltas of all n(n-1)/2 unordered pairs in the reference's linear pair
  * order (index 0 = (1,2), (1,3), ..., (1,n), (2,3), ...), written to the host
  * array out.  Replaces calculateSwapDeltasKernel + its D2H copy
