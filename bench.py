@@ -34,6 +34,8 @@ sys.path.insert(0, os.path.join(ROOT, "brain-match_b200"))
 WORKLOADS = {
     "n18524_e5m": dict(n=18524, e=5_000_000, wmax=30000, tail_prob=1e-3, seed=20261204),
     "n1000_e20k": dict(n=1000, e=20_000, wmax=5000, tail_prob=0.0, seed=20261203),
+    # smaller pair for ncu captures (S = 268 MB, still above L2)
+    "n8192_e1m": dict(n=8192, e=1_000_000, wmax=30000, tail_prob=1e-3, seed=20261206),
 }
 OWN_KERNELS_PER_SWEEP = 9  # relabel x4, row_work, profit, combine, candidates, commit
 CUB_KERNELS_PER_SWEEP = 2 * 9  # two 64-bit radix sorts (1 histogram + 8 passes each)

@@ -90,6 +90,7 @@ def lib():
         L.bm_triple_round.argtypes = [vp, C.POINTER(TripleOpts), C.POINTER(TripleStats)]
         L.bm_timer_mark.argtypes = [vp, i32]
         L.bm_timer_elapsed.argtypes = [vp, i32, i32, C.POINTER(C.c_float)]
+        L.bm_measure_peaks.argtypes = [i32, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.bm_free.argtypes = [vp]
         L.bm_free.restype = None
         L.bm_read_graph_csv.argtypes = [C.c_char_p, C.POINTER(i64), C.POINTER(vp), C.POINTER(vp),
@@ -280,3 +281,10 @@ def write_mapping_csv(path, m, numeric=False):
     m = np.ascontiguousarray(m, np.int32)
     f = lib().bm_write_mapping_csv_numeric if numeric else lib().bm_write_mapping_csv
     _check(f(path.encode(), len(m) - 1, _p(m)))
+
+
+def measure_peaks(n):
+    """(shared-memory atomic adds/s, int32 min+add pairs/s) on the current device."""
+    r, m = C.c_double(), C.c_double()
+    _check(lib().bm_measure_peaks(int(n), C.byref(r), C.byref(m)))
+    return r.value, m.value

@@ -16,6 +16,7 @@
 #include "bm.h"
 #include "bm_kernels.cuh"
 #include "bm_triples.cuh"
+#include "bm_select.cuh"
 
 using namespace bm;
 
@@ -56,6 +57,8 @@ struct bm_ctx {
     cudaEvent_t ev[6] = {};
     cudaEvent_t uev[8] = {};       // bm_timer_* slots
     unsigned long long* work_sum = nullptr;
+    unsigned long long* part = nullptr;   // per-tile best partners (combine)
+    int* pold = nullptr;                  // pre-move images of moved vertices (commit)
 };
 
 static thread_local char g_create_err[512];
@@ -193,6 +196,8 @@ static void free_ctx(bm_ctx* c) {
     for (auto& e : c->ev) if (e) cudaEventDestroy(e);
     for (auto& e : c->uev) if (e) cudaEventDestroy(e);
     if (c->work_sum) cudaFree(c->work_sum);
+    if (c->part) cudaFree(c->part);
+    if (c->pold) cudaFree(c->pold);
     if (c->st) cudaStreamDestroy(c->st);
     delete c;
 }
@@ -493,10 +498,26 @@ static bm_status stage_profit(bm_ctx* ctx) {
 
 static bm_status stage_combine(bm_ctx* ctx, int* all_out) {
     const int n = ctx->n;
-    CK(cudaMemsetAsync(ctx->rowbest, 0, n * sizeof(unsigned long long), ctx->st));
-    const int t = (n + 31) / 32;
-    dim3 grid(t, t), block(32, 8);
-    k_combine<<<grid, block, 0, ctx->st>>>(ctx->S, n, ctx->rowbest, all_out);
+    const int t = (n + kTile - 1) / kTile;
+    if (!ctx->part) CK(dalloc(ctx, &ctx->part, (size_t)t * n * sizeof(unsigned long long)));
+    dim3 grid(t, t);
+    k_combine64<<<grid, 256, 0, ctx->st>>>(ctx->S, n, ctx->part, all_out);
+    CK(cudaGetLastError());
+    k_best_reduce<<<(n + 255) / 256, 256, 0, ctx->st>>>(ctx->part, n, t, ctx->rowbest);
+    CK(cudaGetLastError());
+    return BM_OK;
+}
+
+// G1 adjacency bitmap (x -> y), built once on first use.
+template <bool W16>
+static bm_status ensure_adj(bm_ctx* ctx) {
+    if (ctx->adj) return BM_OK;
+    const int n = ctx->n;
+    ctx->adj_words = (n + 31) / 32;
+    const size_t bytes = (size_t)n * ctx->adj_words * sizeof(unsigned);
+    CK(dalloc(ctx, &ctx->adj, bytes));
+    CK(cudaMemsetAsync(ctx->adj, 0, bytes, ctx->st));
+    k_adj_bits<W16><<<(n + 7) / 8, 256, 0, ctx->st>>>(view<W16>(ctx), ctx->adj, ctx->adj_words);
     CK(cudaGetLastError());
     return BM_OK;
 }
@@ -509,12 +530,14 @@ static bm_status stage_commit(bm_ctx* ctx, const bm_sweep_opts* o) {
     CK(cudaGetLastError());
     size_t tb = ctx->cub_bytes;
     CK(cub::DeviceRadixSort::SortKeys(ctx->cub_tmp, tb, ctx->ckeys, ctx->ckeys_sorted, n, 0, 64, ctx->st));
-    const size_t smem = 2 * (size_t)n;
-    CK(cudaFuncSetAttribute(k_commit<W16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (!ctx->pold) CK(dalloc(ctx, &ctx->pold, (size_t)(n + 1) * sizeof(int)));
     const int max_scan = o ? o->max_candidates : 0;
     const int max_verify = o ? o->max_verify : -1;
-    k_commit<W16><<<1, 1024, smem, ctx->st>>>(view<W16>(ctx), ctx->ckeys_sorted, n, max_scan, max_verify,
-                                               ctx->cstats, nullptr);
+    const int lim = (max_scan > 0 && max_scan < n) ? max_scan : n;
+    const size_t smem = (size_t)n;
+    CK(cudaFuncSetAttribute(k_commit_seq<W16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_commit_seq<W16><<<1, 1024, smem, ctx->st>>>(view<W16>(ctx), ctx->ckeys_sorted, lim, max_verify, ctx->pold,
+                                                  ctx->cstats);
     CK(cudaGetLastError());
     return BM_OK;
 }
@@ -720,14 +743,8 @@ static bm_status triple_round_impl(bm_ctx* ctx, const bm_triple_opts* o, bm_trip
     if (partners > 32768) { set_err(ctx, "bm_triple_round: partners=%d above 32768", partners); return BM_E_INPUT; }
     bm_status s = ensure_S(ctx);
     if (s) return s;
-    if (!ctx->adj) {
-        ctx->adj_words = (n + 31) / 32;
-        const size_t bytes = (size_t)n * ctx->adj_words * sizeof(unsigned);
-        CK(dalloc(ctx, &ctx->adj, bytes));
-        CK(cudaMemsetAsync(ctx->adj, 0, bytes, ctx->st));
-        k_adj_bits<W16><<<(n + 7) / 8, 256, 0, ctx->st>>>(view<W16>(ctx), ctx->adj, ctx->adj_words);
-        CK(cudaGetLastError());
-    }
+    s = ensure_adj<W16>(ctx);
+    if (s) return s;
     if (!ctx->tcount) CK(dalloc(ctx, &ctx->tcount, 2 * sizeof(unsigned long long)));
     const long long before = ctx->score;
     CK(cudaEventRecord(ctx->ev[0], ctx->st));

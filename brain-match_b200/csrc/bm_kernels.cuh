@@ -118,62 +118,85 @@ __global__ void k_row_work(DevView<W16> g, unsigned long long* __restrict__ key,
 // Profit rows.  Persistent CTAs take rows from `order` (heaviest first) via an
 // atomic counter, accumulate the row in shared memory (n+1 ints: slot n
 // absorbs terms for unmatched G2 vertices) and write it to S[a][0..n).
+// Inside a row, warps take the row's G1 edges round robin and scatter the
+// matching G2 list; lists longer than kLongList are queued and then scattered
+// by the whole CTA, so a few hub lists cannot hold the row's barrier.
+constexpr int kLongList = 2048;
+constexpr int kLongQueue = 512;
+
+// Scatters min(w1, w2) over list[i0, i1) into acc, lanes striding by `step`.
+template <bool W16>
+__device__ __forceinline__ void scatter_list(int* acc, const typename Ent<W16>::T* __restrict__ list,
+                                             int i0, int i1, int w1, int first, int step) {
+    typedef Ent<W16> EN;
+    typedef typename EN::T E;
+    int i = i0 + first;
+    for (; i + 3 * step < i1; i += 4 * step) {
+        const E x0 = list[i], x1 = list[i + step], x2 = list[i + 2 * step], x3 = list[i + 3 * step];
+        atomicAdd(&acc[EN::id(x0)], imin(w1, EN::w(x0)));
+        atomicAdd(&acc[EN::id(x1)], imin(w1, EN::w(x1)));
+        atomicAdd(&acc[EN::id(x2)], imin(w1, EN::w(x2)));
+        atomicAdd(&acc[EN::id(x3)], imin(w1, EN::w(x3)));
+    }
+    for (; i < i1; i += step) { const E x = list[i]; atomicAdd(&acc[EN::id(x)], imin(w1, EN::w(x))); }
+}
+
 template <bool W16>
 __global__ void __launch_bounds__(512)
 k_profit(DevView<W16> g, const int* __restrict__ order, int* __restrict__ counter) {
     typedef Ent<W16> EN;
     typedef typename EN::T E;
     extern __shared__ int acc[];
-    __shared__ int s_row;
+    __shared__ int s_row, s_nlong;
+    __shared__ int2 s_long[kLongQueue];  // (G2 vertex, w1 | kind << 31)
     const int n = g.n;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
     for (;;) {
-        if (tid == 0) s_row = atomicAdd(counter, 1);
+        if (tid == 0) { s_row = atomicAdd(counter, 1); s_nlong = 0; }
         __syncthreads();
         const int r = s_row;
         if (r >= n) break;
         const int a = order[r];
         for (int i = tid; i <= n; i += blockDim.x) acc[i] = 0;
         __syncthreads();
-        // out-edges of a against G2 in-lists of p(v)
-        {
-            const int s0 = g.off1o[a], s1 = g.off1o[a + 1];
-            for (int j = s0 + wid; j < s1; j += nw) {
-                const E ea = g.ent1oP[j];
-                const int f = EN::id(ea), w1 = EN::w(ea);
-                const int b0 = g.off2i[f], b1 = g.off2i[f + 1];
-                int i = b0 + lane;
-                for (; i + 32 < b1; i += 64) {
-                    const E x = g.ent2iP[i], y = g.ent2iP[i + 32];
-                    atomicAdd(&acc[EN::id(x)], imin(w1, EN::w(x)));
-                    atomicAdd(&acc[EN::id(y)], imin(w1, EN::w(y)));
+        // out-edges of a against G2 in-lists of p(v), then in-edges against out-lists of p(u)
+        const int so = g.off1o[a], lo = g.off1o[a + 1] - so;
+        const int si = g.off1i[a], li = g.off1i[a + 1] - si;
+        for (int j = wid; j < lo + li; j += nw) {
+            const bool out = j < lo;
+            const E ea = out ? g.ent1oP[so + j] : g.ent1iP[si + (j - lo)];
+            const int f = EN::id(ea), w1 = EN::w(ea);
+            const int* off = out ? g.off2i : g.off2o;
+            const E* list = out ? g.ent2iP : g.ent2oP;
+            const int b0 = off[f], b1 = off[f + 1];
+            if (b1 - b0 > kLongList) {
+                int q = 0;
+                if (lane == 0) q = atomicAdd(&s_nlong, 1);
+                q = __shfl_sync(0xffffffffu, q, 0);
+                if (q < kLongQueue) {
+                    if (lane == 0) s_long[q] = make_int2(f, w1 | (out ? 0 : (int)0x80000000));
+                    continue;
                 }
-                if (i < b1) { const E x = g.ent2iP[i]; atomicAdd(&acc[EN::id(x)], imin(w1, EN::w(x))); }
             }
+            scatter_list<W16>(acc, list, b0, b1, w1, lane, 32);
         }
-        // in-edges of a against G2 out-lists of p(u)
-        {
-            const int s0 = g.off1i[a], s1 = g.off1i[a + 1];
-            for (int j = s0 + wid; j < s1; j += nw) {
-                const E ea = g.ent1iP[j];
-                const int f = EN::id(ea), w1 = EN::w(ea);
-                const int b0 = g.off2o[f], b1 = g.off2o[f + 1];
-                int i = b0 + lane;
-                for (; i + 32 < b1; i += 64) {
-                    const E x = g.ent2oP[i], y = g.ent2oP[i + 32];
-                    atomicAdd(&acc[EN::id(x)], imin(w1, EN::w(x)));
-                    atomicAdd(&acc[EN::id(y)], imin(w1, EN::w(y)));
-                }
-                if (i < b1) { const E x = g.ent2oP[i]; atomicAdd(&acc[EN::id(x)], imin(w1, EN::w(x))); }
-            }
+        __syncthreads();
+        // long lists, one at a time, by the whole CTA
+        const int nl = min(s_nlong, kLongQueue);
+        for (int q = 0; q < nl; q++) {
+            const int2 e = s_long[q];
+            const bool out = e.y >= 0;
+            const int w1 = e.y & 0x7fffffff;
+            const int* off = out ? g.off2i : g.off2o;
+            const E* list = out ? g.ent2iP : g.ent2oP;
+            scatter_list<W16>(acc, list, off[e.x], off[e.x + 1], w1, tid, blockDim.x);
         }
         // corner corrections for every G1 edge a->b
         {
             const int pa = g.p[a];
-            const int s0 = g.off1o[a], s1 = g.off1o[a + 1];
-            for (int j = s0 + tid; j < s1; j += blockDim.x) {
-                const int b = EN::id(g.ent1o[j]);
-                const E ep = g.ent1oP[j];
+            for (int j = tid; j < lo; j += blockDim.x) {
+                const int b = EN::id(g.ent1o[so + j]);
+                const E ep = g.ent1oP[so + j];
                 const int pb = EN::id(ep), x = EN::w(ep);
                 const int c = imin(x, g.w2(pa, pb)) + imin(x, g.w2(pb, pa))
                             - imin(x, g.w2(pa, pa)) - imin(x, g.w2(pb, pb));
@@ -184,6 +207,7 @@ k_profit(DevView<W16> g, const int* __restrict__ order, int* __restrict__ counte
         {
             const int q0 = g.offs[a], q1 = g.offs[a + 1];
             if (q1 > q0) {
+                __syncthreads();
                 for (int b = tid; b < n; b += blockDim.x) {
                     const int pb = g.p[b];
                     const int d = g.w2(pb, pb);
@@ -207,65 +231,13 @@ k_profit(DevView<W16> g, const int* __restrict__ order, int* __restrict__ counte
 }
 
 // ---------------------------------------------------------------------------
-// Pair combine.  32x32 tiles of the upper triangle: delta(a,b) for a<b from
-// S[a][b], S[b][a] and the diagonal.  Keeps, per row, the best partner as a
-// packed key  (delta + 2^31) << 32 | ~b  (larger delta, then smaller b, wins)
-// and optionally writes every delta at the reference's linear pair index.
+// Per-row best partner as a packed key  (delta + 2^31) << 32 | ~b  (larger
+// delta, then smaller b, wins).
 __device__ __forceinline__ unsigned long long pack_best(int d, int b) {
     return ((unsigned long long)(unsigned)(d + 0x80000000u) << 32) | (unsigned)(~b);
 }
 __device__ __forceinline__ unsigned long long kmax(unsigned long long x, unsigned long long y) {
     return x > y ? x : y;
-}
-
-__global__ void __launch_bounds__(256)
-k_combine(const int* __restrict__ S, int n, unsigned long long* __restrict__ rowbest,
-          int* __restrict__ all_out) {
-    __shared__ int sA[32][33];  // S[a0+r][b0+c]
-    __shared__ int sB[32][33];  // S[b0+r][a0+c]
-    __shared__ int dA[32], dB[32];
-    __shared__ unsigned long long colbest[8][32];
-    const int ti = blockIdx.y, tj = blockIdx.x;
-    if (ti > tj) return;
-    const int a0 = ti * 32, b0 = tj * 32;
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    for (int r = ty; r < 32; r += 8) {
-        const int a = a0 + r, b = b0 + tx;
-        sA[r][tx] = (a < n && b < n) ? S[(size_t)a * n + b] : 0;
-        const int bb = b0 + r, aa = a0 + tx;
-        sB[r][tx] = (bb < n && aa < n) ? S[(size_t)bb * n + aa] : 0;
-    }
-    if (ty == 0) {
-        const int a = a0 + tx, b = b0 + tx;
-        dA[tx] = a < n ? S[(size_t)a * n + a] : 0;
-        dB[tx] = b < n ? S[(size_t)b * n + b] : 0;
-    }
-    __syncthreads();
-    const int b = b0 + tx;
-    unsigned long long cb = 0;  // best partner a for row b
-    for (int r = ty; r < 32; r += 8) {
-        const int a = a0 + r;
-        const bool ok = (a < b) && (b < n);
-        int d = 0;
-        if (ok) {
-            d = sA[r][tx] + sB[tx][r] - dA[r] - dB[tx];
-            if (all_out) {
-                const long long idx = (long long)a * (2LL * n - a - 1) / 2 + (b - a - 1);
-                all_out[idx] = d;
-            }
-            cb = kmax(cb, pack_best(d, a));
-        }
-        unsigned long long rk = ok ? pack_best(d, b) : 0ull;
-        for (int o = 16; o; o >>= 1) rk = kmax(rk, __shfl_xor_sync(0xffffffffu, rk, o));
-        if (tx == 0 && rk) atomicMax(&rowbest[a], rk);
-    }
-    colbest[ty][tx] = cb;
-    __syncthreads();
-    if (ty == 0) {
-        unsigned long long k = colbest[0][tx];
-        for (int y = 1; y < 8; y++) k = kmax(k, colbest[y][tx]);
-        if (k && b < n) atomicMax(&rowbest[b], k);
-    }
 }
 
 // Candidate keys: one per row whose best partner improves, deduplicated when
@@ -388,91 +360,10 @@ __global__ void k_score(DevView<W16> g, unsigned long long* __restrict__ out) {
 }
 
 // ---------------------------------------------------------------------------
-// Sequential commit of sorted candidates (one CTA).
-//   used[x]  : x already moved in this sweep
-//   taint[x] : x is a G1 neighbour of a moved vertex, so its cached delta may
-//              be stale and must be re-evaluated before committing.
-// A candidate whose endpoints are untainted keeps its sweep delta exactly,
-// because a swap delta depends only on p at the two endpoints and at their
-// G1 neighbours.
+// Counters reported by the commit kernels.
 struct CommitStats {
     long long total_delta;
     int scanned, verified, committed, pad;
 };
-
-template <bool W16>
-__global__ void __launch_bounds__(1024)
-k_commit(DevView<W16> g, const unsigned long long* __restrict__ keys, int nkeys,
-         int max_scan, int max_verify, CommitStats* __restrict__ st, int* __restrict__ moves) {
-    typedef Ent<W16> EN;
-    extern __shared__ unsigned char flags[];  // used[n] then taint[n]
-    unsigned char* used = flags;
-    unsigned char* taint = flags + g.n;
-    __shared__ int red[32];
-    __shared__ int s_delta;
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    for (int i = tid; i < 2 * g.n; i += blockDim.x) flags[i] = 0;
-    long long total = 0;
-    int scanned = 0, verified = 0, committed = 0;
-    __syncthreads();
-    const int lim = (max_scan > 0 && max_scan < nkeys) ? max_scan : nkeys;
-    for (int k = 0; k < lim; k++) {
-        const unsigned long long key = keys[k];
-        if (key == ~0ull) break;
-        const int lo = (int)((key >> 16) & 0xffffu), hi = (int)(key & 0xffffu);
-        const int d0 = (int)(0x7fffffffu - (unsigned)(key >> 32));
-        scanned++;
-        if (used[lo] | used[hi]) continue;
-        int d = d0;
-        if (taint[lo] | taint[hi]) {
-            if (max_verify >= 0 && verified >= max_verify) continue;
-            verified++;
-            int part = swap_delta_part<W16>(g, lo, hi, tid, blockDim.x);
-            for (int o = 16; o; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
-            if (lane == 0) red[wid] = part;
-            __syncthreads();
-            if (wid == 0) {
-                int v = lane < (blockDim.x >> 5) ? red[lane] : 0;
-                for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-                if (lane == 0) s_delta = v;
-            }
-            __syncthreads();
-            d = s_delta;
-            __syncthreads();
-        }
-        if (d <= 0) continue;
-        if (tid == 0) {
-            const int flo = g.p[lo], fhi = g.p[hi];
-            g.p[lo] = fhi; g.p[hi] = flo;
-            if (fhi < g.n) g.pinv[fhi] = lo;
-            if (flo < g.n) g.pinv[flo] = hi;
-            used[lo] = 1; used[hi] = 1;
-            if (moves) { moves[3 * committed] = lo; moves[3 * committed + 1] = hi; moves[3 * committed + 2] = d; }
-        }
-        total += d;
-        committed++;
-        // taint the G1 neighbourhoods of both endpoints
-        const int l0 = g.off1o[lo], l1 = g.off1o[lo + 1] - l0;
-        const int i0 = g.off1i[lo], i1 = g.off1i[lo + 1] - i0;
-        const int m0 = g.off1o[hi], m1 = g.off1o[hi + 1] - m0;
-        const int j0 = g.off1i[hi], j1 = g.off1i[hi + 1] - j0;
-        const int tot = l1 + i1 + m1 + j1;
-        for (int q = tid; q < tot; q += blockDim.x) {
-            int r = q, x;
-            if (r < l1) x = EN::id(g.ent1o[l0 + r]);
-            else if ((r -= l1) < i1) x = EN::id(g.ent1i[i0 + r]);
-            else if ((r -= i1) < m1) x = EN::id(g.ent1o[m0 + r]);
-            else { r -= m1; x = EN::id(g.ent1i[j0 + r]); }
-            taint[x] = 1;
-        }
-        __syncthreads();
-    }
-    if (tid == 0) {
-        st->total_delta = total;
-        st->scanned = scanned;
-        st->verified = verified;
-        st->committed = committed;
-    }
-}
 
 }  // namespace bm

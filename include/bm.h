@@ -221,6 +221,15 @@ bm_status bm_first_improvement(bm_ctx* ctx, int32_t max_passes, int64_t* commits
 bm_status bm_timer_mark(bm_ctx* ctx, int32_t slot);
 bm_status bm_timer_elapsed(bm_ctx* ctx, int32_t start_slot, int32_t end_slot, float* ms);
 
+/*
+ * Microbenchmarks behind the sweep's roofline figures, on the current device:
+ * *red_per_s = shared-memory atomic adds per second at random addresses of an
+ * n-int array at full occupancy (the profit-row kernel's inner operation);
+ * *minadd_per_s = independent int32 (min, add) pairs per second.
+ * Allocates a 4-byte scratch word; diagnostic, not on the hot path.
+ */
+bm_status bm_measure_peaks(int32_t n, double* red_per_s, double* minadd_per_s);
+
 /* ---- 3-cycles ---- */
 
 /*
