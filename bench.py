@@ -37,8 +37,8 @@ WORKLOADS = {
     # smaller pair for ncu captures (S = 268 MB, still above L2)
     "n8192_e1m": dict(n=8192, e=1_000_000, wmax=30000, tail_prob=1e-3, seed=20261206),
 }
-OWN_KERNELS_PER_SWEEP = 9  # relabel x4, row_work, profit, combine, candidates, commit
-CUB_KERNELS_PER_SWEEP = 2 * 9  # two 64-bit radix sorts (1 histogram + 8 passes each)
+OWN_KERNELS_PER_SWEEP = 13  # relabel x5, row_work, hub B build, hub GEMM, profit, combine + reduce, candidates, commit
+CUB_KERNELS_PER_SWEEP = 20  # two 64-bit radix sorts: histogram + exclusive sum + 8 onesweep passes each
 
 
 def peaks():
@@ -274,8 +274,107 @@ def run_engine(args, g, world, rank, local, pg):
             "gpu_launches": args.steps * (OWN_KERNELS_PER_SWEEP + CUB_KERNELS_PER_SWEEP),
             "clocks": clk.summary(),
             "sweeps": [{k: s[k] for k in ("score_before", "score_after", "committed", "verified", "candidates",
-                                         "ms_prep", "ms_profit", "ms_combine", "ms_commit", "ms_total",
-                                         "min_terms")} for s in stats],
+                                         "ms_prep", "ms_hub", "ms_profit", "ms_combine", "ms_commit",
+                                         "ms_total", "min_terms", "commit_entries", "commit_steps",
+                                         "commit_carried")} for s in stats],
+        }
+        print(json.dumps(line), flush=True)
+    E.close()
+
+
+def batch_pairs(seed=20261207, count=64):
+    """64 instances, N log-uniform in [500, 8000], E = 20 N, weights as the N=1,000 workload."""
+    import bm
+    rng = np.random.default_rng(seed)
+    ns = np.exp(rng.uniform(np.log(500), np.log(8000), count)).astype(int)
+    return [bm.generate(bm.gen_params(n=int(n), e=20 * int(n), seed=seed + 1 + i)) for i, n in enumerate(ns)]
+
+
+def run_batch(args, world, rank, local, pg):
+    import bm
+    import torch
+    torch.cuda.set_device(local)
+    pairs = batch_pairs(20261207 + 1000 * rank)
+    B = bm.Batch(pairs)
+    info = B.info()
+    B.set_mappings([g["map0"] for g in pairs])
+    pt, tile = B.autotune()
+    B.sweeps(args.warmup)
+    barrier(pg)
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        commits, ms = B.sweeps(args.steps)
+        torch.cuda.synchronize()
+    barrier(pg)
+    ms_max = allreduce_max(pg, ms)
+    value = world * args.steps * info["total_pairs"] / (ms_max / 1e3)
+    maps = B.get_mappings()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        B.set_mappings(maps)
+        B.sweeps(1)
+        maps = B.get_mappings()
+    e2e_s = allreduce_max(pg, time.perf_counter() - t0)
+    if rank == 0:
+        h2d = sum(2 * (g["n"] + 1) * 4 for g in pairs)
+        line = {
+            "metric": "exact swap deltas/s (batched instances)", "value": value, "unit": "deltas/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "config": {"workload": "batch64", "instances": info["count"], "max_n": info["max_n"],
+                       "pairs_per_step": info["total_pairs"], "edges": "20 N per instance",
+                       "autotuned": {"profit_threads": pt, "combine_tile": tile},
+                       "step": "one sweep of every instance (CUDA graph replay)", "parallelism": f"replicas{world}"},
+            "e2e": {"value": world * args.steps * info["total_pairs"] / e2e_s, "unit": "deltas/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d // 2},
+            "committed_last_steps": int(commits.sum()),
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    B.close()
+
+
+def run_triples(args, world, rank, local, pg):
+    """3-cycle rounds on the N=18,524 pair, starting from the pairwise sweep's
+    output matching (50 sweeps, untimed): 256 two-hop partners per vertex,
+    both rotations of every triple evaluated exactly, best disjoint set
+    committed."""
+    import bm
+    import torch
+    torch.cuda.set_device(local)
+    p = dict(WORKLOADS["n18524_e5m"])
+    p["seed"] += rank
+    g = bm.generate(bm.gen_params(**p))
+    E = bm.Engine.from_pair(g)
+    E.set_mapping(g["map0"])
+    for _ in range(args.pre_sweeps):
+        if E.sweep()["committed"] == 0:
+            break
+    start_score = E.score()
+    for r in range(args.warmup):
+        E.triple_round(partners=256, seed=1000 + r)
+    barrier(pg)
+    torch.cuda.synchronize()
+    stats = []
+    with Clocks(local) as clk:
+        E.timer_mark(0)
+        for r in range(args.steps):
+            stats.append(E.triple_round(partners=256, seed=2000 + r))
+        E.timer_mark(1)
+        torch.cuda.synchronize()
+    barrier(pg)
+    ms = allreduce_max(pg, E.timer_elapsed(0, 1))
+    rot = sum(s["rotations"] for s in stats)
+    if rank == 0:
+        line = {
+            "metric": "exact 3-cycle rotation deltas/s", "value": world * rot / (ms / 1e3), "unit": "rotations/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "config": {"workload": "triples_n18524", "partners": 256, "pre_sweeps": args.pre_sweeps,
+                       "start_score": start_score, "step": "one 3-cycle round"},
+            "rounds": [{k: s[k] for k in ("triples", "committed", "verified", "score_after", "ms_sample",
+                                         "ms_eval", "ms_commit", "ms_total")} for s in stats],
+            "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)
     E.close()
@@ -287,12 +386,19 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--workload", default="n18524_e5m", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="n18524_e5m", choices=sorted(WORKLOADS) + ["batch64", "triples"])
+    ap.add_argument("--pre-sweeps", type=int, default=50)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     world, rank, local, pg = dist_setup()
     import bm
+    if args.workload in ("batch64", "triples"):
+        (run_batch if args.workload == "batch64" else run_triples)(args, world, rank, local, pg)
+        if pg is not None:
+            pg.barrier()
+            pg.destroy_process_group()
+        return
     p = dict(WORKLOADS[args.workload])
     p["seed"] += rank  # independent replica per rank
     g = bm.generate(bm.gen_params(**p))

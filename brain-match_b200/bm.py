@@ -15,6 +15,7 @@ LIB_PATH = os.path.join(_HERE, "lib", "libbm.so")
 BM_OK, BM_E_INPUT, BM_E_CUDA, BM_E_OVERFLOW, BM_E_TIMEOUT, BM_E_NOMEM, BM_E_STATE, BM_E_IO = (
     0, -1, -2, -3, -4, -5, -6, -7)
 BM_FLAG_FORCE_I32 = 1
+BM_FLAG_NO_HUB_GEMM = 2
 BM_STATIC_MAX_PAIRS = 65536
 
 
@@ -28,7 +29,7 @@ class GenParams(C.Structure):
 class Info(C.Structure):
     _fields_ = [("n", C.c_int32), ("entry_bits", C.c_int32), ("e1", C.c_int64), ("e2", C.c_int64),
                 ("g1_self_loops", C.c_int64), ("device_bytes", C.c_int64), ("device", C.c_int32),
-                ("num_sms", C.c_int32)]
+                ("num_sms", C.c_int32), ("hubs", C.c_int32), ("hub_k", C.c_int32)]
 
 
 class SweepOpts(C.Structure):
@@ -40,7 +41,8 @@ class SweepStats(C.Structure):
                 ("candidates", C.c_int32), ("scanned", C.c_int32), ("verified", C.c_int32),
                 ("committed", C.c_int32), ("best_delta", C.c_int32), ("reserved", C.c_int32),
                 ("ms_profit", C.c_float), ("ms_combine", C.c_float), ("ms_commit", C.c_float),
-                ("ms_total", C.c_float), ("ms_prep", C.c_float), ("pad", C.c_int32), ("min_terms", C.c_int64)]
+                ("ms_total", C.c_float), ("ms_prep", C.c_float), ("ms_hub", C.c_float), ("min_terms", C.c_int64),
+                ("commit_entries", C.c_int64), ("commit_steps", C.c_int32), ("commit_carried", C.c_int32)]
 
 
 class TripleOpts(C.Structure):
@@ -91,6 +93,17 @@ def lib():
         L.bm_timer_mark.argtypes = [vp, i32]
         L.bm_timer_elapsed.argtypes = [vp, i32, i32, C.POINTER(C.c_float)]
         L.bm_measure_peaks.argtypes = [i32, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.bm_batch_create.argtypes = [C.POINTER(vp), i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, u32]
+        L.bm_batch_destroy.argtypes = [vp]
+        L.bm_batch_destroy.restype = None
+        L.bm_batch_last_error.restype = C.c_char_p
+        L.bm_batch_last_error.argtypes = [vp]
+        L.bm_batch_set_mappings.argtypes = [vp, vp]
+        L.bm_batch_get_mappings.argtypes = [vp, vp]
+        L.bm_batch_scores.argtypes = [vp, vp]
+        L.bm_batch_autotune.argtypes = [vp, C.POINTER(i32), C.POINTER(i32)]
+        L.bm_batch_sweeps.argtypes = [vp, i32, C.POINTER(SweepOpts), vp, C.POINTER(C.c_float)]
+        L.bm_batch_info.argtypes = [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(i64), C.POINTER(i32), C.POINTER(i32)]
         L.bm_free.argtypes = [vp]
         L.bm_free.restype = None
         L.bm_read_graph_csv.argtypes = [C.c_char_p, C.POINTER(i64), C.POINTER(vp), C.POINTER(vp),
@@ -226,7 +239,7 @@ class Engine:
         o = SweepOpts(max_candidates, max_verify)
         s = SweepStats()
         _check(lib().bm_sweep(self.h, C.byref(o), C.byref(s)), self.h)
-        return {k: getattr(s, k) for k, _ in SweepStats._fields_ if k not in ("reserved", "pad")}
+        return {k: getattr(s, k) for k, _ in SweepStats._fields_ if k != "reserved"}
 
     def timer_mark(self, slot):
         _check(lib().bm_timer_mark(self.h, slot), self.h)
@@ -288,3 +301,85 @@ def measure_peaks(n):
     r, m = C.c_double(), C.c_double()
     _check(lib().bm_measure_peaks(int(n), C.byref(r), C.byref(m)))
     return r.value, m.value
+
+
+class Batch:
+    """Independent instances swept together (bm_batch_*)."""
+
+    def __init__(self, pairs, flags=0):
+        self.pairs = pairs
+        k = len(pairs)
+        keep = []
+
+        def arr(key):
+            xs = [np.ascontiguousarray(g[key], np.int32) for g in pairs]
+            keep.extend(xs)
+            ptrs = (C.c_void_p * k)(*[x.ctypes.data for x in xs])
+            keep.append(ptrs)
+            return ptrs
+        n = np.array([g["n"] for g in pairs], np.int32)
+        e1 = np.array([len(g["src1"]) for g in pairs], np.int64)
+        e2 = np.array([len(g["src2"]) for g in pairs], np.int64)
+        keep += [n, e1, e2]
+        h = C.c_void_p()
+        st = lib().bm_batch_create(C.byref(h), k, _p(n), _p(e1), arr("src1"), arr("dst1"), arr("w1"),
+                                   _p(e2), arr("src2"), arr("dst2"), arr("w2"), flags)
+        if st != BM_OK:
+            raise BMError(st, (lib().bm_batch_last_error(None) or b"").decode())
+        self.h = h
+        self.k = k
+        self.ns = [int(g["n"]) for g in pairs]
+
+    def _chk(self, st):
+        if st != BM_OK:
+            raise BMError(st, (lib().bm_batch_last_error(self.h) or b"").decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().bm_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_mappings(self, maps):
+        ms = [np.ascontiguousarray(m, np.int32) for m in maps]
+        ptrs = (C.c_void_p * self.k)(*[m.ctypes.data for m in ms])
+        self._chk(lib().bm_batch_set_mappings(self.h, ptrs))
+
+    def get_mappings(self):
+        ms = [np.zeros(n + 1, np.int32) for n in self.ns]
+        ptrs = (C.c_void_p * self.k)(*[m.ctypes.data for m in ms])
+        self._chk(lib().bm_batch_get_mappings(self.h, ptrs))
+        return ms
+
+    def scores(self):
+        s = np.zeros(self.k, np.int64)
+        self._chk(lib().bm_batch_scores(self.h, _p(s)))
+        return s
+
+    def autotune(self):
+        a, b = C.c_int32(), C.c_int32()
+        self._chk(lib().bm_batch_autotune(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def sweeps(self, k, max_candidates=0, max_verify=-1):
+        o = SweepOpts(max_candidates, max_verify)
+        c = np.zeros(self.k, np.int64)
+        ms = C.c_float()
+        self._chk(lib().bm_batch_sweeps(self.h, int(k), C.byref(o), _p(c), C.byref(ms)))
+        return c, ms.value
+
+    def info(self):
+        vals = [C.c_int32(), C.c_int32(), C.c_int64(), C.c_int32(), C.c_int32()]
+        self._chk(lib().bm_batch_info(self.h, *[C.byref(v) for v in vals]))
+        return dict(zip(("count", "max_n", "total_pairs", "profit_threads", "combine_tile"), [v.value for v in vals]))

@@ -1,0 +1,580 @@
+// bm_batch.cu -- many independent alignment instances of uneven size swept
+// together.
+//
+// Each instance is an ordinary context (bm_create: same preprocessing, same
+// storage, same exact arithmetic); the batch adds device tables of the
+// instances' buffers and batched kernels that run the shared per-row,
+// per-tile and per-instance bodies of the single-instance path:
+//   relabel (all lists of all instances)  -> row work + one LPT sort over all
+//   (instance, row) items -> one persistent profit-row launch over every item
+//   -> one combine launch over every (instance, tile) item -> reduce ->
+//   candidates -> one segmented sort -> one commit launch (a CTA per instance)
+//   -> per-instance statistics.
+// One sweep of the whole batch is captured once as a CUDA graph and replayed.
+// The launch shapes (profit-row block size, combine tile) are picked by
+// bm_batch_autotune, which times the candidates on the batch itself; results
+// do not depend on the choice.  Hub tensor-core terms are not used here: the
+// instances are built with BM_FLAG_NO_HUB_GEMM.
+#include <cstdio>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+#include <cuda_runtime.h>
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_segmented_radix_sort.cuh>
+#include "bm.h"
+#include "bm_internal.cuh"
+#include "bm_select.cuh"
+
+namespace {
+
+// Per-instance device record of the batch.
+struct BatchInst {
+    int n;
+    int tiles;            // combine tiles per side for the current tile size
+    long long tile_base;  // first global (instance, tile) item
+    int row_base;         // first global (instance, row) item / candidate slot
+    int* S;
+    unsigned long long* rowbest;
+    unsigned long long* part;
+    unsigned long long* keys;
+    unsigned long long* keys_sorted;
+};
+
+__device__ __forceinline__ int find_inst(const int* __restrict__ base, int nb, long long it) {
+    int lo = 0, hi = nb;  // base[lo] <= it < base[hi]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (base[mid] <= it) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+__device__ __forceinline__ int find_inst_ll(const long long* __restrict__ base, int nb, long long it) {
+    int lo = 0, hi = nb;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (base[mid] <= it) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+template <bool W16>
+__global__ void k_b_relabel(const DevView<W16>* __restrict__ views, const long long* __restrict__ e1,
+                            const long long* __restrict__ e2, const typename Ent<W16>::T* const* __restrict__ src,
+                            int nb) {
+    typedef Ent<W16> EN;
+    const int b = blockIdx.y;
+    const DevView<W16> g = views[b];
+    // lists: 0 G1 out, 1 G1 in (through p); 2 G2 out, 3 G2 in (through pinv)
+    const int lst = blockIdx.z;
+    const long long m = lst < 2 ? e1[b] : e2[b];
+    const typename EN::T* in = src[4 * b + lst];
+    typename EN::T* out = lst == 0 ? g.ent1oP : lst == 1 ? g.ent1iP : lst == 2 ? g.ent2oP : g.ent2iP;
+    const int* map = lst < 2 ? g.p : g.pinv;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (long long)gridDim.x * blockDim.x) {
+        const typename EN::T e = in[i];
+        out[i] = EN::make(map[EN::id(e)], EN::w(e));
+    }
+}
+
+template <bool W16>
+__global__ void k_b_row_work(const DevView<W16>* __restrict__ views, const int* __restrict__ row_base, int nb,
+                             int total, unsigned long long* __restrict__ key, int* __restrict__ val) {
+    typedef Ent<W16> EN;
+    const int lane = threadIdx.x & 31;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int it = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; it < total; it += nwarps) {
+        const int b = find_inst(row_base, nb, it);
+        const DevView<W16>& g = views[b];
+        const int a = it - row_base[b];
+        long long w = 0;
+        for (int i = g.off1o[a] + lane; i < g.off1o[a + 1]; i += 32) {
+            const int f = EN::id(g.ent1oP[i]);
+            w += g.off2i[f + 1] - g.off2i[f];
+        }
+        for (int i = g.off1i[a] + lane; i < g.off1i[a + 1]; i += 32) {
+            const int f = EN::id(g.ent1iP[i]);
+            w += g.off2o[f + 1] - g.off2o[f];
+        }
+        for (int o = 16; o; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+        if (lane == 0) {
+            w += (g.off1o[a + 1] - g.off1o[a]) + (g.off1i[a + 1] - g.off1i[a]) + 64;
+            if (g.offs[a + 1] > g.offs[a]) w += g.n;
+            key[it] = (unsigned long long)w;
+            val[it] = it;
+        }
+    }
+}
+
+template <bool W16>
+__global__ void __launch_bounds__(512)
+k_b_profit(const DevView<W16>* __restrict__ views, const int* __restrict__ row_base, int nb, int total,
+           const int* __restrict__ order, int* __restrict__ counter) {
+    extern __shared__ int acc[];
+    __shared__ int s_item, s_nlong;
+    __shared__ int2 s_long[kLongQueue];
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+        __syncthreads();
+        const int r = s_item;
+        if (r >= total) break;
+        const int it = order[r];
+        const int b = find_inst(row_base, nb, it);
+        const DevView<W16> g = views[b];
+        profit_row<W16>(g, it - row_base[b], acc, s_long, &s_nlong, nullptr, 0);
+    }
+}
+
+// (instance, tile) items: the upper triangle of each instance, row-major.
+template <int T>
+__global__ void __launch_bounds__(256)
+k_b_combine(const BatchInst* __restrict__ inst, const long long* __restrict__ tile_base, int nb, long long total) {
+    for (long long it = blockIdx.x; it < total; it += gridDim.x) {
+        const int b = find_inst_ll(tile_base, nb, it);
+        const BatchInst I = inst[b];
+        long long t = it - tile_base[b];
+        int ti = 0;
+        while (t >= I.tiles - ti) { t -= I.tiles - ti; ti++; }
+        const int tj = ti + (int)t;
+        combine_tile<T>(I.S, I.n, ti, tj, I.part, nullptr);
+        __syncthreads();
+    }
+}
+
+__global__ void k_b_reduce(const BatchInst* __restrict__ inst, int nb) {
+    const int b = blockIdx.y;
+    const BatchInst I = inst[b];
+    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < I.n; x += gridDim.x * blockDim.x) {
+        unsigned long long k = 0;
+        for (int t = 0; t < I.tiles; t++) k = kmax(k, I.part[(size_t)t * I.n + x]);
+        I.rowbest[x] = k;
+    }
+}
+
+// Candidate keys of every instance (the single-instance rule, k_candidates).
+__global__ void k_b_candidates(const BatchInst* __restrict__ inst, int nb) {
+    const int b = blockIdx.y;
+    const BatchInst I = inst[b];
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < I.n; a += gridDim.x * blockDim.x) {
+        const unsigned long long k = I.rowbest[a];
+        unsigned long long out = ~0ull;
+        if (k) {
+            const int d = (int)((unsigned)(k >> 32) - 0x80000000u);
+            const int p = (int)(~(unsigned)(k & 0xffffffffu));
+            if (d > 0) {
+                const unsigned long long kb = I.rowbest[p];
+                const int pp = (int)(~(unsigned)(kb & 0xffffffffu));
+                const bool mutual = (kb != 0) && (pp == a);
+                if (!mutual || a < p) {
+                    const int lo = a < p ? a : p, hi = a < p ? p : a;
+                    out = ((unsigned long long)(0x7fffffffu - (unsigned)d) << 32) |
+                          ((unsigned long long)lo << 16) | (unsigned long long)hi;
+                }
+            }
+        }
+        I.keys[a] = out;
+    }
+}
+
+template <bool W16>
+__global__ void __launch_bounds__(1024)
+k_b_commit(const DevView<W16>* __restrict__ views, const BatchInst* __restrict__ inst, int max_scan,
+           int max_verify, CommitStats* __restrict__ st, long long* __restrict__ acc_delta,
+           long long* __restrict__ acc_commits) {
+    extern __shared__ unsigned char smem[];
+    const int b = blockIdx.x;
+    const DevView<W16> g = views[b];
+    const BatchInst I = inst[b];
+    const int lim = (max_scan > 0 && max_scan < I.n) ? max_scan : I.n;
+    commit_group<W16>(g, I.keys_sorted, lim, max_verify, &st[b], smem);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        acc_delta[b] += st[b].total_delta;
+        acc_commits[b] += st[b].committed;
+    }
+}
+
+}  // namespace
+
+struct bm_batch {
+    int count = 0, max_n = 0, total = 0;
+    bool w16 = true;
+    std::vector<bm_ctx*> ctx;
+    cudaStream_t st = nullptr;
+    char err[512] = {0};
+    // tuning
+    int profit_threads = 512, tile = 64;
+    bool tuned = false;
+    // device tables
+    void* views = nullptr;                // DevView<W16>[count]
+    BatchInst* inst = nullptr;
+    int* row_base = nullptr;              // count+1
+    long long* tile_base = nullptr;       // count+1
+    long long *e1 = nullptr, *e2 = nullptr;
+    void** lists = nullptr;               // 4 per instance: ent1o, ent1i, ent2o, ent2i
+    unsigned long long *wkeys = nullptr, *wkeys_sorted = nullptr, *ckeys = nullptr, *ckeys_sorted = nullptr;
+    int *wvals = nullptr, *order = nullptr;
+    unsigned long long *rowbest = nullptr, *part = nullptr;
+    void* cub_tmp = nullptr;
+    size_t cub_bytes = 0;
+    int* counter = nullptr;
+    CommitStats* cstats = nullptr;
+    long long *acc_delta = nullptr, *acc_commits = nullptr;
+    long long total_tiles = 0;
+    std::vector<BatchInst> hinst;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int graph_max_scan = 0, graph_max_verify = -1;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+static thread_local char g_batch_create_err[512];
+
+#define BK(call)                                                                         \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess) {                                                         \
+            snprintf(B->err, sizeof B->err, "%s:%d: %s: %s", __FILE__, __LINE__, #call,  \
+                     cudaGetErrorString(e_));                                            \
+            return BM_E_CUDA;                                                            \
+        }                                                                                \
+    } while (0)
+
+static void batch_free(bm_batch* B) {
+    if (!B) return;
+    if (B->exec) cudaGraphExecDestroy(B->exec);
+    if (B->graph) cudaGraphDestroy(B->graph);
+    void* bufs[] = {B->views, B->inst, B->row_base, B->tile_base, B->e1, B->e2, B->lists, B->wkeys,
+                    B->wkeys_sorted, B->ckeys, B->ckeys_sorted, B->wvals, B->order, B->rowbest, B->part,
+                    B->cub_tmp, B->counter, B->cstats, B->acc_delta, B->acc_commits};
+    for (void* p : bufs) if (p) cudaFree(p);
+    if (B->ev0) cudaEventDestroy(B->ev0);
+    if (B->ev1) cudaEventDestroy(B->ev1);
+    if (B->st) cudaStreamDestroy(B->st);
+    for (bm_ctx* c : B->ctx) bm_destroy(c);
+    delete B;
+}
+
+extern "C" void bm_batch_destroy(bm_batch* B) { batch_free(B); }
+extern "C" const char* bm_batch_last_error(const bm_batch* B) { return B ? B->err : g_batch_create_err; }
+
+// (Re)builds the per-instance tile tables for the current tile size.
+static bm_status batch_tiles(bm_batch* B) {
+    std::vector<long long> tb(B->count + 1, 0);
+    for (int i = 0; i < B->count; i++) {
+        const int T = (B->hinst[i].n + B->tile - 1) / B->tile;
+        B->hinst[i].tiles = T;
+        B->hinst[i].tile_base = tb[i];
+        tb[i + 1] = tb[i] + (long long)T * (T + 1) / 2;
+    }
+    B->total_tiles = tb[B->count];
+    BK(cudaMemcpy(B->tile_base, tb.data(), tb.size() * sizeof(long long), cudaMemcpyHostToDevice));
+    BK(cudaMemcpy(B->inst, B->hinst.data(), B->hinst.size() * sizeof(BatchInst), cudaMemcpyHostToDevice));
+    return BM_OK;
+}
+
+template <bool W16>
+static bm_status batch_tables(bm_batch* B) {
+    std::vector<DevView<W16>> v(B->count);
+    std::vector<void*> lists(4 * B->count);
+    std::vector<long long> e1(B->count), e2(B->count);
+    for (int i = 0; i < B->count; i++) {
+        v[i] = view<W16>(B->ctx[i]);
+        lists[4 * i + 0] = B->ctx[i]->ent1o;
+        lists[4 * i + 1] = B->ctx[i]->ent1i;
+        lists[4 * i + 2] = B->ctx[i]->ent2o;
+        lists[4 * i + 3] = B->ctx[i]->ent2i;
+        e1[i] = B->ctx[i]->e1;
+        e2[i] = B->ctx[i]->e2;
+    }
+    BK(cudaMalloc(&B->views, v.size() * sizeof(DevView<W16>)));
+    BK(cudaMemcpy(B->views, v.data(), v.size() * sizeof(DevView<W16>), cudaMemcpyHostToDevice));
+    BK(cudaMalloc(&B->lists, lists.size() * sizeof(void*)));
+    BK(cudaMemcpy(B->lists, lists.data(), lists.size() * sizeof(void*), cudaMemcpyHostToDevice));
+    BK(cudaMalloc(&B->e1, B->count * sizeof(long long)));
+    BK(cudaMalloc(&B->e2, B->count * sizeof(long long)));
+    BK(cudaMemcpy(B->e1, e1.data(), B->count * sizeof(long long), cudaMemcpyHostToDevice));
+    BK(cudaMemcpy(B->e2, e2.data(), B->count * sizeof(long long), cudaMemcpyHostToDevice));
+    return BM_OK;
+}
+
+extern "C" bm_status bm_batch_create(bm_batch** out, int32_t count, const int32_t* n, const int64_t* e1,
+                                     const int32_t* const* src1, const int32_t* const* dst1,
+                                     const int32_t* const* w1, const int64_t* e2, const int32_t* const* src2,
+                                     const int32_t* const* dst2, const int32_t* const* w2, uint32_t flags) {
+    if (!out || count < 1 || !n || !e1 || !src1 || !dst1 || !w1 || !e2 || !src2 || !dst2 || !w2)
+        return BM_E_INPUT;
+    *out = nullptr;
+    bm_batch* B = new (std::nothrow) bm_batch();
+    if (!B) return BM_E_NOMEM;
+    B->count = count;
+    // every instance in one storage mode
+    const uint32_t f = (flags | BM_FLAG_NO_HUB_GEMM);
+    bool any32 = (flags & BM_FLAG_FORCE_I32) != 0;
+    for (int pass = 0; pass < 2; pass++) {
+        for (bm_ctx* c : B->ctx) bm_destroy(c);
+        B->ctx.clear();
+        for (int i = 0; i < count; i++) {
+            bm_ctx* c = nullptr;
+            bm_status s = bm_create(&c, n[i], e1[i], src1[i], dst1[i], w1[i], e2[i], src2[i], dst2[i], w2[i],
+                                    f | (any32 ? BM_FLAG_FORCE_I32 : 0u));
+            if (s != BM_OK) {
+                snprintf(g_batch_create_err, sizeof g_batch_create_err, "instance %d: %s", i, bm_last_error(nullptr));
+                batch_free(B);
+                return s;
+            }
+            B->ctx.push_back(c);
+        }
+        bool mixed = false;
+        for (bm_ctx* c : B->ctx) mixed |= !c->w16;
+        if (!mixed || any32) break;
+        any32 = true;  // some instance needs 32-bit entries: rebuild all that way
+    }
+    B->w16 = B->ctx[0]->w16;
+    bm_status s;
+    for (bm_ctx* c : B->ctx) {
+        if ((s = ensure_S(c)) != BM_OK) {
+            snprintf(g_batch_create_err, sizeof g_batch_create_err, "%s", c->err);
+            batch_free(B);
+            return s;
+        }
+        B->max_n = std::max(B->max_n, c->n);
+        B->total += c->n;
+    }
+    auto body = [&]() -> bm_status {
+        BK(cudaStreamCreateWithFlags(&B->st, cudaStreamNonBlocking));
+        BK(cudaEventCreate(&B->ev0));
+        BK(cudaEventCreate(&B->ev1));
+        // concatenated per-instance buffers, sized for the smallest tile (32)
+        std::vector<int> rb(count + 1, 0);
+        long long part_total = 0;
+        for (int i = 0; i < count; i++) {
+            rb[i + 1] = rb[i] + B->ctx[i]->n;
+            part_total += (long long)((B->ctx[i]->n + 31) / 32) * B->ctx[i]->n;
+        }
+        BK(cudaMalloc(&B->row_base, rb.size() * sizeof(int)));
+        BK(cudaMemcpy(B->row_base, rb.data(), rb.size() * sizeof(int), cudaMemcpyHostToDevice));
+        BK(cudaMalloc(&B->tile_base, (count + 1) * sizeof(long long)));
+        BK(cudaMalloc(&B->inst, count * sizeof(BatchInst)));
+        const size_t tot = (size_t)B->total;
+        BK(cudaMalloc(&B->wkeys, tot * sizeof(unsigned long long)));
+        BK(cudaMalloc(&B->wkeys_sorted, tot * sizeof(unsigned long long)));
+        BK(cudaMalloc(&B->ckeys, tot * sizeof(unsigned long long)));
+        BK(cudaMalloc(&B->ckeys_sorted, tot * sizeof(unsigned long long)));
+        BK(cudaMalloc(&B->wvals, tot * sizeof(int)));
+        BK(cudaMalloc(&B->order, tot * sizeof(int)));
+        BK(cudaMalloc(&B->rowbest, tot * sizeof(unsigned long long)));
+        BK(cudaMalloc(&B->part, (size_t)part_total * sizeof(unsigned long long)));
+        BK(cudaMalloc(&B->counter, sizeof(int)));
+        BK(cudaMalloc(&B->cstats, count * sizeof(CommitStats)));
+        BK(cudaMalloc(&B->acc_delta, count * sizeof(long long)));
+        BK(cudaMalloc(&B->acc_commits, count * sizeof(long long)));
+        size_t b1 = 0, b2 = 0;
+        BK(cub::DeviceRadixSort::SortPairsDescending(nullptr, b1, B->wkeys, B->wkeys_sorted, B->wvals, B->order,
+                                                     B->total));
+        BK(cub::DeviceSegmentedRadixSort::SortKeys(nullptr, b2, B->ckeys, B->ckeys_sorted, B->total, count,
+                                                   B->row_base, B->row_base + 1));
+        B->cub_bytes = std::max(b1, b2);
+        BK(cudaMalloc(&B->cub_tmp, B->cub_bytes));
+        B->hinst.resize(count);
+        long long poff = 0;
+        for (int i = 0; i < count; i++) {
+            BatchInst& I = B->hinst[i];
+            I.n = B->ctx[i]->n;
+            I.row_base = rb[i];
+            I.S = B->ctx[i]->S;
+            I.rowbest = B->rowbest + rb[i];
+            I.part = B->part + poff;
+            poff += (long long)((I.n + 31) / 32) * I.n;
+            I.keys = B->ckeys + rb[i];
+            I.keys_sorted = B->ckeys_sorted + rb[i];
+        }
+        bm_status s2 = B->w16 ? batch_tables<true>(B) : batch_tables<false>(B);
+        if (s2) return s2;
+        return batch_tiles(B);
+    };
+    s = body();
+    if (s != BM_OK) {
+        snprintf(g_batch_create_err, sizeof g_batch_create_err, "%s", B->err);
+        batch_free(B);
+        return s;
+    }
+    *out = B;
+    return BM_OK;
+}
+
+extern "C" bm_status bm_batch_set_mappings(bm_batch* B, const int32_t* const* maps) {
+    if (!B || !maps) return BM_E_INPUT;
+    for (int i = 0; i < B->count; i++) {
+        bm_status s = bm_set_mapping(B->ctx[i], maps[i]);
+        if (s) { snprintf(B->err, sizeof B->err, "instance %d: %s", i, B->ctx[i]->err); return s; }
+    }
+    return BM_OK;
+}
+
+extern "C" bm_status bm_batch_get_mappings(bm_batch* B, int32_t* const* maps) {
+    if (!B || !maps) return BM_E_INPUT;
+    for (int i = 0; i < B->count; i++) {
+        bm_status s = bm_get_mapping(B->ctx[i], maps[i]);
+        if (s) { snprintf(B->err, sizeof B->err, "instance %d: %s", i, B->ctx[i]->err); return s; }
+    }
+    return BM_OK;
+}
+
+extern "C" bm_status bm_batch_scores(bm_batch* B, int64_t* scores) {
+    if (!B || !scores) return BM_E_INPUT;
+    for (int i = 0; i < B->count; i++) {
+        bm_status s = bm_score(B->ctx[i], &scores[i]);
+        if (s) { snprintf(B->err, sizeof B->err, "instance %d: %s", i, B->ctx[i]->err); return s; }
+    }
+    return BM_OK;
+}
+
+// Enqueues the profit and combine stages of one batch sweep on B->st.
+template <bool W16>
+static bm_status enqueue_eval(bm_batch* B) {
+    typedef typename Ent<W16>::T E;
+    const DevView<W16>* views = (const DevView<W16>*)B->views;
+    long long maxe = 0;
+    for (bm_ctx* c : B->ctx) maxe = std::max(maxe, std::max(c->e1, c->e2));
+    dim3 rg((unsigned)std::min<long long>((maxe + 255) / 256, 256), B->count, 4);
+    k_b_relabel<W16><<<rg, 256, 0, B->st>>>(views, B->e1, B->e2, (const E* const*)B->lists, B->count);
+    BK(cudaGetLastError());
+    k_b_row_work<W16><<<(B->total + 7) / 8, 256, 0, B->st>>>(views, B->row_base, B->count, B->total, B->wkeys,
+                                                            B->wvals);
+    BK(cudaGetLastError());
+    size_t tb = B->cub_bytes;
+    BK(cub::DeviceRadixSort::SortPairsDescending(B->cub_tmp, tb, B->wkeys, B->wkeys_sorted, B->wvals, B->order,
+                                                 B->total, 0, 64, B->st));
+    BK(cudaMemsetAsync(B->counter, 0, sizeof(int), B->st));
+    const size_t smem = (size_t)(B->max_n + 1) * sizeof(int);
+    BK(cudaFuncSetAttribute(k_b_profit<W16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0, sms = B->ctx[0]->num_sms;
+    BK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_b_profit<W16>, B->profit_threads, smem));
+    if (per_sm < 1) { snprintf(B->err, sizeof B->err, "profit kernel does not fit (max n %d)", B->max_n); return BM_E_INPUT; }
+    k_b_profit<W16><<<sms * per_sm, B->profit_threads, smem, B->st>>>(views, B->row_base, B->count, B->total,
+                                                                     B->order, B->counter);
+    BK(cudaGetLastError());
+    const unsigned cg = (unsigned)std::min<long long>(B->total_tiles, (long long)sms * 16);
+    if (B->tile == 32) k_b_combine<32><<<cg, 256, 0, B->st>>>(B->inst, B->tile_base, B->count, B->total_tiles);
+    else k_b_combine<64><<<cg, 256, 0, B->st>>>(B->inst, B->tile_base, B->count, B->total_tiles);
+    BK(cudaGetLastError());
+    dim3 cg2((B->max_n + 255) / 256, B->count);
+    k_b_reduce<<<cg2, 256, 0, B->st>>>(B->inst, B->count);
+    BK(cudaGetLastError());
+    return BM_OK;
+}
+
+template <bool W16>
+static bm_status enqueue_select_commit(bm_batch* B, int max_scan, int max_verify) {
+    dim3 cg2((B->max_n + 255) / 256, B->count);
+    k_b_candidates<<<cg2, 256, 0, B->st>>>(B->inst, B->count);
+    BK(cudaGetLastError());
+    size_t tb = B->cub_bytes;
+    BK(cub::DeviceSegmentedRadixSort::SortKeys(B->cub_tmp, tb, B->ckeys, B->ckeys_sorted, B->total, B->count,
+                                               B->row_base, B->row_base + 1, 0, 64, B->st));
+    const size_t smem = commit_group_smem(B->max_n);
+    BK(cudaFuncSetAttribute(k_b_commit<W16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_b_commit<W16><<<B->count, 1024, smem, B->st>>>((const DevView<W16>*)B->views, B->inst, max_scan, max_verify,
+                                                     B->cstats, B->acc_delta, B->acc_commits);
+    BK(cudaGetLastError());
+    return BM_OK;
+}
+
+static bm_status enqueue_sweep(bm_batch* B, int max_scan, int max_verify) {
+    bm_status s = B->w16 ? enqueue_eval<true>(B) : enqueue_eval<false>(B);
+    if (s) return s;
+    return B->w16 ? enqueue_select_commit<true>(B, max_scan, max_verify)
+                  : enqueue_select_commit<false>(B, max_scan, max_verify);
+}
+
+extern "C" bm_status bm_batch_autotune(bm_batch* B, int32_t* profit_threads, int32_t* combine_tile) {
+    if (!B) return BM_E_INPUT;
+    for (bm_ctx* c : B->ctx)
+        if (!c->mapped) { snprintf(B->err, sizeof B->err, "bm_batch_autotune: mappings not set"); return BM_E_STATE; }
+    const int pt[2] = {256, 512}, tl[2] = {32, 64};
+    float best = 1e30f;
+    int bp = 512, bt = 64;
+    for (int i = 0; i < 2; i++)
+        for (int j = 0; j < 2; j++) {
+            B->profit_threads = pt[i];
+            B->tile = tl[j];
+            bm_status s = batch_tiles(B);
+            if (s) return s;
+            float ms = 0, tot = 0;
+            for (int rep = 0; rep < 3; rep++) {
+                BK(cudaEventRecord(B->ev0, B->st));
+                s = B->w16 ? enqueue_eval<true>(B) : enqueue_eval<false>(B);
+                if (s) return s;
+                BK(cudaEventRecord(B->ev1, B->st));
+                BK(cudaEventSynchronize(B->ev1));
+                BK(cudaEventElapsedTime(&ms, B->ev0, B->ev1));
+                if (rep) tot += ms;  // first repetition warms up
+            }
+            if (tot < best) { best = tot; bp = pt[i]; bt = tl[j]; }
+        }
+    B->profit_threads = bp;
+    B->tile = bt;
+    bm_status s = batch_tiles(B);
+    if (s) return s;
+    B->tuned = true;
+    if (B->exec) { cudaGraphExecDestroy(B->exec); B->exec = nullptr; }
+    if (B->graph) { cudaGraphDestroy(B->graph); B->graph = nullptr; }
+    if (profit_threads) *profit_threads = bp;
+    if (combine_tile) *combine_tile = bt;
+    return BM_OK;
+}
+
+extern "C" bm_status bm_batch_sweeps(bm_batch* B, int32_t sweeps, const bm_sweep_opts* opts,
+                                     int64_t* committed, float* ms) {
+    if (!B || sweeps < 0) return BM_E_INPUT;
+    for (bm_ctx* c : B->ctx)
+        if (!c->mapped) { snprintf(B->err, sizeof B->err, "bm_batch_sweeps: mappings not set"); return BM_E_STATE; }
+    const int max_scan = opts ? opts->max_candidates : 0;
+    const int max_verify = opts ? opts->max_verify : -1;
+    // one sweep of the whole batch as a CUDA graph, captured once per option set
+    if (B->exec && (max_scan != B->graph_max_scan || max_verify != B->graph_max_verify)) {
+        cudaGraphExecDestroy(B->exec); B->exec = nullptr;
+        cudaGraphDestroy(B->graph); B->graph = nullptr;
+    }
+    if (!B->exec) {
+        BK(cudaStreamBeginCapture(B->st, cudaStreamCaptureModeThreadLocal));
+        bm_status s = enqueue_sweep(B, max_scan, max_verify);
+        cudaGraph_t g = nullptr;
+        cudaError_t ce = cudaStreamEndCapture(B->st, &g);
+        if (s) { if (g) cudaGraphDestroy(g); return s; }
+        BK(ce);
+        B->graph = g;
+        BK(cudaGraphInstantiate(&B->exec, B->graph, 0));
+        B->graph_max_scan = max_scan;
+        B->graph_max_verify = max_verify;
+    }
+    BK(cudaMemsetAsync(B->acc_delta, 0, B->count * sizeof(long long), B->st));
+    BK(cudaMemsetAsync(B->acc_commits, 0, B->count * sizeof(long long), B->st));
+    BK(cudaEventRecord(B->ev0, B->st));
+    for (int i = 0; i < sweeps; i++) BK(cudaGraphLaunch(B->exec, B->st));
+    BK(cudaEventRecord(B->ev1, B->st));
+    std::vector<long long> dsum(B->count), csum(B->count);
+    BK(cudaMemcpyAsync(dsum.data(), B->acc_delta, B->count * sizeof(long long), cudaMemcpyDeviceToHost, B->st));
+    BK(cudaMemcpyAsync(csum.data(), B->acc_commits, B->count * sizeof(long long), cudaMemcpyDeviceToHost, B->st));
+    BK(cudaStreamSynchronize(B->st));
+    for (int i = 0; i < B->count; i++) {
+        B->ctx[i]->score += dsum[i];
+        if (committed) committed[i] = csum[i];
+    }
+    if (ms) BK(cudaEventElapsedTime(ms, B->ev0, B->ev1));
+    return BM_OK;
+}
+
+extern "C" bm_status bm_batch_info(const bm_batch* B, int32_t* count, int32_t* max_n, int64_t* total_pairs,
+                                   int32_t* profit_threads, int32_t* combine_tile) {
+    if (!B) return BM_E_INPUT;
+    long long pairs = 0;
+    for (bm_ctx* c : B->ctx) pairs += (long long)c->n * (c->n - 1) / 2;
+    if (count) *count = B->count;
+    if (max_n) *max_n = B->max_n;
+    if (total_pairs) *total_pairs = pairs;
+    if (profit_threads) *profit_threads = B->profit_threads;
+    if (combine_tile) *combine_tile = B->tile;
+    return BM_OK;
+}

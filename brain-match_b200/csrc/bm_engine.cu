@@ -14,78 +14,21 @@
 #include <cuda_runtime.h>
 #include <cub/device/device_radix_sort.cuh>
 #include "bm.h"
-#include "bm_kernels.cuh"
+#include "bm_internal.cuh"
 #include "bm_triples.cuh"
 #include "bm_select.cuh"
+#include "bm_hub.cuh"
 
 using namespace bm;
 
-struct bm_ctx {
-    int n = 0;
-    bool w16 = true;
-    int dev = 0, num_sms = 0;
-    long long e1 = 0, e2 = 0, nself = 0;
-    cudaStream_t st = nullptr;
-    char err[512] = {0};
-    bool mapped = false;
-    long long score = 0;  // score of the current matching (kept exact across commits)
-    // device buffers
-    int *off1o = nullptr, *off1i = nullptr, *off2o = nullptr, *off2i = nullptr, *offs = nullptr, *selfw = nullptr;
-    void *ent1o = nullptr, *ent1i = nullptr, *ent2o = nullptr, *ent2i = nullptr;
-    void *ent1oP = nullptr, *ent1iP = nullptr, *ent2oP = nullptr, *ent2iP = nullptr;
-    void* W2 = nullptr;
-    int *p = nullptr, *pinv = nullptr;
-    int* S = nullptr;
-    unsigned long long* rowbest = nullptr;
-    unsigned long long *ckeys = nullptr, *ckeys_sorted = nullptr;
-    unsigned long long *wkeys = nullptr, *wkeys_sorted = nullptr;
-    int *wvals = nullptr, *order = nullptr;
-    void* cub_tmp = nullptr;
-    size_t cub_bytes = 0;
-    int* small = nullptr;          // [0]=row counter [1]=ncand [2]=best delta
-    unsigned long long* score_acc = nullptr;
-    CommitStats* cstats = nullptr;
-    int* scratch_pairs = nullptr;  // pair/triple inputs and outputs (ints)
-    long long scratch_cap = 0;
-    unsigned* adj = nullptr;       // G1 adjacency bitmap (3-cycles)
-    int adj_words = 0;
-    int* rowd = nullptr;           // reference-order row deltas
-    int* first = nullptr;          // [0] = first improving partner, [1] = copy for the host
-    long long* fi_acc = nullptr;   // [0] = delta sum, [1] = commits
-    unsigned long long* tcount = nullptr;
-    long long dev_bytes = 0;
-    cudaEvent_t ev[6] = {};
-    cudaEvent_t uev[8] = {};       // bm_timer_* slots
-    unsigned long long* work_sum = nullptr;
-    unsigned long long* part = nullptr;   // per-tile best partners (combine)
-    int* pold = nullptr;                  // pre-move images of moved vertices (commit)
-};
-
 static thread_local char g_create_err[512];
 
-static void set_err(bm_ctx* c, const char* fmt, ...) {
+void set_err(bm_ctx* c, const char* fmt, ...) {
     char* dst = c ? c->err : g_create_err;
     va_list ap;
     va_start(ap, fmt);
     vsnprintf(dst, 512, fmt, ap);
     va_end(ap);
-}
-
-#define CK(call)                                                                   \
-    do {                                                                           \
-        cudaError_t e_ = (call);                                                   \
-        if (e_ != cudaSuccess) {                                                   \
-            set_err(ctx, "%s:%d: %s: %s", __FILE__, __LINE__, #call,               \
-                    cudaGetErrorString(e_));                                       \
-            return BM_E_CUDA;                                                      \
-        }                                                                          \
-    } while (0)
-
-template <typename T>
-static cudaError_t dalloc(bm_ctx* ctx, T** ptr, size_t bytes) {
-    cudaError_t e = cudaMalloc((void**)ptr, bytes ? bytes : 16);
-    if (e == cudaSuccess) ctx->dev_bytes += (long long)bytes;
-    return e;
 }
 
 extern "C" const char* bm_last_error(const bm_ctx* ctx) { return ctx ? ctx->err : g_create_err; }
@@ -123,25 +66,6 @@ static void build_csr(int n, const std::vector<int>& key, const std::vector<int>
 }  // namespace
 
 template <bool W16>
-static DevView<W16> view(bm_ctx* c) {
-    DevView<W16> g;
-    typedef typename Ent<W16>::T E;
-    typedef typename Dense<W16>::T D;
-    g.n = c->n;
-    g.off1o = c->off1o; g.ent1o = (const E*)c->ent1o;
-    g.off1i = c->off1i; g.ent1i = (const E*)c->ent1i;
-    g.off2o = c->off2o; g.ent2o = (const E*)c->ent2o;
-    g.off2i = c->off2i; g.ent2i = (const E*)c->ent2i;
-    g.offs = c->offs; g.selfw = c->selfw;
-    g.ent1oP = (E*)c->ent1oP; g.ent1iP = (E*)c->ent1iP;
-    g.ent2oP = (E*)c->ent2oP; g.ent2iP = (E*)c->ent2iP;
-    g.W2 = (const D*)c->W2;
-    g.p = c->p; g.pinv = c->pinv;
-    g.S = c->S;
-    return g;
-}
-
-template <bool W16>
 static bm_status upload_lists(bm_ctx* ctx, const HostCSR& g1o, const HostCSR& g1i,
                               const HostCSR& g2o, const HostCSR& g2i, int clamp1, int clamp2) {
     typedef Ent<W16> EN;
@@ -163,30 +87,49 @@ static bm_status upload_lists(bm_ctx* ctx, const HostCSR& g1o, const HostCSR& g1
 }
 
 template <bool W16>
-static bm_status upload_dense(bm_ctx* ctx, const HostCSR& g2o, int clamp2) {
+static bm_status upload_entries(bm_ctx* ctx, const HostCSR& h, void** dst, void** dstP) {
+    typedef Ent<W16> EN;
+    typedef typename EN::T E;
+    std::vector<E> v(h.id.size());
+    for (size_t i = 0; i < v.size(); i++) v[i] = EN::make(h.id[i], h.w[i]);
+    CK(dalloc(ctx, (E**)dst, v.size() * sizeof(E)));
+    CK(dalloc(ctx, (E**)dstP, v.size() * sizeof(E)));
+    if (!v.empty()) CK(cudaMemcpy(*dst, v.data(), v.size() * sizeof(E), cudaMemcpyHostToDevice));
+    return BM_OK;
+}
+
+template <bool W16>
+static bm_status upload_dense(bm_ctx* ctx, const HostCSR& g2o, const HostCSR& g2i, int clamp2) {
     typedef typename Dense<W16>::T D;
     const size_t n1 = (size_t)ctx->n + 1;
-    CK(dalloc(ctx, (D**)&ctx->W2, n1 * n1 * sizeof(D)));
-    CK(cudaMemset(ctx->W2, 0, n1 * n1 * sizeof(D)));
-    // fill row by row through a pinned staging row
-    std::vector<D> row(n1);
     const int n = ctx->n;
+    CK(dalloc(ctx, (D**)&ctx->W2, n1 * n1 * sizeof(D)));
+    CK(dalloc(ctx, (D**)&ctx->W2T, n1 * n1 * sizeof(D)));
+    CK(cudaMemset(ctx->W2, 0, n1 * n1 * sizeof(D)));
+    CK(cudaMemset(ctx->W2T, 0, n1 * n1 * sizeof(D)));
+    // fill row by row (and the transpose column by column) through a staging buffer
     const size_t chunk_rows = 256;
     std::vector<D> buf(chunk_rows * n1);
-    for (int f0 = 0; f0 < n; f0 += (int)chunk_rows) {
-        const int f1 = std::min(n, f0 + (int)chunk_rows);
-        std::fill(buf.begin(), buf.end(), (D)0);
-        for (int f = f0; f < f1; f++)
-            for (int i = g2o.off[f]; i < g2o.off[f + 1]; i++)
-                buf[(size_t)(f - f0) * n1 + g2o.id[i]] = (D)std::min(g2o.w[i], clamp2);
-        CK(cudaMemcpy((D*)ctx->W2 + (size_t)f0 * n1, buf.data(), (size_t)(f1 - f0) * n1 * sizeof(D),
-                      cudaMemcpyHostToDevice));
+    for (int t = 0; t < 2; t++) {
+        for (int f0 = 0; f0 < n; f0 += (int)chunk_rows) {
+            const int f1 = std::min(n, f0 + (int)chunk_rows);
+            std::fill(buf.begin(), buf.end(), (D)0);
+            const HostCSR& h = t == 0 ? g2o : g2i;  // in-lists are the rows of the transpose
+            for (int f = f0; f < f1; f++)
+                for (int i = h.off[f]; i < h.off[f + 1]; i++)
+                    buf[(size_t)(f - f0) * n1 + h.id[i]] = (D)std::min(h.w[i], clamp2);
+            D* out = (D*)(t == 0 ? ctx->W2 : ctx->W2T);
+            CK(cudaMemcpy(out + (size_t)f0 * n1, buf.data(), (size_t)(f1 - f0) * n1 * sizeof(D),
+                          cudaMemcpyHostToDevice));
+        }
     }
     return BM_OK;
 }
 
 static void free_ctx(bm_ctx* c) {
     if (!c) return;
+    for (void* b : {(void*)c->off2oH, c->ent2oH, c->ent2oHP}) if (b) cudaFree(b);
+    if (c->W2T) cudaFree(c->W2T);
     void* bufs[] = {c->off1o, c->off1i, c->off2o, c->off2i, c->offs, c->selfw, c->ent1o, c->ent1i,
                     c->ent2o, c->ent2i, c->ent1oP, c->ent1iP, c->ent2oP, c->ent2iP, c->W2, c->p,
                     c->pinv, c->S, c->rowbest, c->ckeys, c->ckeys_sorted, c->wkeys, c->wkeys_sorted,
@@ -197,7 +140,9 @@ static void free_ctx(bm_ctx* c) {
     for (auto& e : c->uev) if (e) cudaEventDestroy(e);
     if (c->work_sum) cudaFree(c->work_sum);
     if (c->part) cudaFree(c->part);
-    if (c->pold) cudaFree(c->pold);
+    for (void* b : {(void*)c->hubs, (void*)c->is_hub, (void*)c->hubA, (void*)c->hubB, (void*)c->hub_err})
+        if (b) cudaFree(b);
+    if (c->ev_hub) cudaEventDestroy(c->ev_hub);
     if (c->st) cudaStreamDestroy(c->st);
     delete c;
 }
@@ -316,10 +261,62 @@ extern "C" bm_status bm_create(bm_ctx** out, int32_t n, int64_t e1, const int32_
         s = w16 ? upload_lists<true>(ctx, g1o, g1i, g2o, g2i, clamp1, clamp2)
                 : upload_lists<false>(ctx, g1o, g1i, g2o, g2i, clamp1, clamp2);
         if (s) return s;
-        s = w16 ? upload_dense<true>(ctx, g2o, clamp2) : upload_dense<false>(ctx, g2o, clamp2);
+        s = w16 ? upload_dense<true>(ctx, g2o, g2i, clamp2) : upload_dense<false>(ctx, g2o, g2i, clamp2);
         if (s) return s;
+        {   // G2 out-entries above the hub threshold (hub residual terms)
+            HostCSR hv;
+            hv.off.assign((size_t)n + 2, 0);
+            for (int f = 0; f < n; f++) {
+                int c = 0;
+                for (int i = g2o.off[f]; i < g2o.off[f + 1]; i++) c += g2o.w[i] > kHubT;
+                hv.off[f + 1] = hv.off[f] + c;
+            }
+            hv.off[n + 1] = hv.off[n];
+            for (int f = 0; f < n; f++)
+                for (int i = g2o.off[f]; i < g2o.off[f + 1]; i++)
+                    if (g2o.w[i] > kHubT) { hv.id.push_back(g2o.id[i]); hv.w.push_back(std::min(g2o.w[i], clamp2)); }
+            ctx->e2H = (long long)hv.id.size();
+            if ((s = up_off(hv, &ctx->off2oH))) return s;
+            s = w16 ? upload_entries<true>(ctx, hv, &ctx->ent2oH, &ctx->ent2oHP)
+                    : upload_entries<false>(ctx, hv, &ctx->ent2oH, &ctx->ent2oHP);
+            if (s) return s;
+        }
         CK(dalloc(ctx, &ctx->p, (n + 1) * sizeof(int)));
         CK(dalloc(ctx, &ctx->pinv, (n + 1) * sizeof(int)));
+        CK(cudaEventCreate(&ctx->ev_hub));
+        CK(dalloc(ctx, &ctx->hub_err, sizeof(int)));
+        CK(cudaMemset(ctx->hub_err, 0, sizeof(int)));
+        if (!(flags & BM_FLAG_NO_HUB_GEMM)) {
+            // hubs: G1 vertices of out-degree >= max(64, n/8), at most kHubMaxHubs,
+            // topped up by the next-largest out-degrees to a multiple of 16 so the
+            // GEMM depth (hubs x thresholds) is a multiple of 128 bytes
+            std::vector<int> byd(n);
+            for (int v = 0; v < n; v++) byd[v] = v;
+            std::stable_sort(byd.begin(), byd.end(), [&](int x, int y) {
+                return (g1o.off[x + 1] - g1o.off[x]) > (g1o.off[y + 1] - g1o.off[y]);
+            });
+            const int thr = std::max(64, n / 8);
+            int nh = 0;
+            while (nh < std::min(n, kHubMaxHubs) && g1o.off[byd[nh] + 1] - g1o.off[byd[nh]] >= thr) nh++;
+            if (nh > 0) {
+                nh = std::min(std::min(n, kHubMaxHubs), (nh + 15) / 16 * 16);
+                if (nh % 16 == 0) {
+                    std::vector<unsigned char> flag(n, 0);
+                    std::vector<int> hv(byd.begin(), byd.begin() + nh);
+                    for (int v : hv) flag[v] = 1;
+                    ctx->nh = nh;
+                    ctx->hubK = nh * kHubT;
+                    ctx->Mpad = (n + kGemmM - 1) / kGemmM * kGemmM;
+                    ctx->Npad = (n + kGemmN - 1) / kGemmN * kGemmN;
+                    CK(dalloc(ctx, &ctx->hubs, nh * sizeof(int)));
+                    CK(cudaMemcpy(ctx->hubs, hv.data(), nh * sizeof(int), cudaMemcpyHostToDevice));
+                    CK(dalloc(ctx, &ctx->is_hub, n));
+                    CK(cudaMemcpy(ctx->is_hub, flag.data(), n, cudaMemcpyHostToDevice));
+                    CK(dalloc(ctx, &ctx->hubA, (size_t)ctx->Mpad * ctx->hubK));
+                    CK(dalloc(ctx, &ctx->hubB, (size_t)ctx->Npad * ctx->hubK));
+                }
+            }
+        }
         CK(dalloc(ctx, &ctx->rowbest, n * sizeof(unsigned long long)));
         CK(dalloc(ctx, &ctx->ckeys, n * sizeof(unsigned long long)));
         CK(dalloc(ctx, &ctx->ckeys_sorted, n * sizeof(unsigned long long)));
@@ -355,6 +352,8 @@ extern "C" bm_status bm_get_info(const bm_ctx* ctx, bm_info* info) {
     info->device_bytes = ctx->dev_bytes;
     info->device = ctx->dev;
     info->num_sms = ctx->num_sms;
+    info->hubs = ctx->nh;
+    info->hub_k = ctx->hubK;
     return BM_OK;
 }
 
@@ -459,7 +458,7 @@ extern "C" bm_status bm_pair_deltas(bm_ctx* ctx, int64_t k, const int32_t* m1, c
 
 // ---------------------------------------------------------------------------
 // Sweep stages.
-static bm_status ensure_S(bm_ctx* ctx) {
+bm_status ensure_S(bm_ctx* ctx) {
     if (ctx->S) return BM_OK;
     CK(dalloc(ctx, &ctx->S, (size_t)ctx->n * ctx->n * sizeof(int)));
     return BM_OK;
@@ -475,22 +474,43 @@ static bm_status stage_profit(bm_ctx* ctx) {
     k_relabel<W16><<<rb, 256, 0, ctx->st>>>((const E*)ctx->ent1i, (E*)ctx->ent1iP, ctx->e1, ctx->p);
     k_relabel<W16><<<rb, 256, 0, ctx->st>>>((const E*)ctx->ent2o, (E*)ctx->ent2oP, ctx->e2, ctx->pinv);
     k_relabel<W16><<<rb, 256, 0, ctx->st>>>((const E*)ctx->ent2i, (E*)ctx->ent2iP, ctx->e2, ctx->pinv);
+    if (ctx->nh && ctx->e2H)
+        k_relabel<W16><<<rb, 256, 0, ctx->st>>>((const E*)ctx->ent2oH, (E*)ctx->ent2oHP, ctx->e2H, ctx->pinv);
     CK(cudaGetLastError());
     // heaviest rows first
     CK(cudaMemsetAsync(ctx->work_sum, 0, sizeof(unsigned long long), ctx->st));
-    k_row_work<W16><<<(n + 7) / 8, 256, 0, ctx->st>>>(g, ctx->wkeys, ctx->wvals, ctx->work_sum);
+    k_row_work<W16><<<(n + 7) / 8, 256, 0, ctx->st>>>(g, ctx->is_hub, ctx->wkeys, ctx->wvals, ctx->work_sum);
     CK(cudaGetLastError());
     size_t tb = ctx->cub_bytes;
     CK(cub::DeviceRadixSort::SortPairsDescending(ctx->cub_tmp, tb, ctx->wkeys, ctx->wkeys_sorted,
                                                  ctx->wvals, ctx->order, n, 0, 64, ctx->st));
     CK(cudaMemsetAsync(ctx->small, 0, sizeof(int), ctx->st));
+    CK(cudaEventRecord(ctx->ev_hub, ctx->st));
+    if (ctx->nh) {
+        // hub in-edge terms up to the threshold: one exact u8 GEMM on the tensor cores into S
+        const int K = ctx->hubK;
+        if (!ctx->hubA_built) {
+            CK(cudaMemsetAsync(ctx->hubA, 0, (size_t)ctx->Mpad * K, ctx->st));
+            k_hub_build_A<W16><<<ctx->nh, 256, 0, ctx->st>>>(g, ctx->hubs, ctx->nh, K, ctx->hubA);
+            CK(cudaGetLastError());
+            ctx->hubA_built = true;
+        }
+        CK(cudaMemsetAsync(ctx->hubB, 0, (size_t)ctx->Npad * K, ctx->st));
+        k_hub_build_B<W16><<<ctx->nh, 256, 0, ctx->st>>>(g, ctx->hubs, ctx->nh, K, ctx->hubB);
+        CK(cudaGetLastError());
+        CK(cudaFuncSetAttribute(k_hub_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem));
+        dim3 grid(ctx->Npad / kGemmN, ctx->Mpad / kGemmM);
+        k_hub_gemm<<<grid, kGemmThreads, kGemmSmem, ctx->st>>>(ctx->hubA, ctx->hubB, K, n, ctx->S, ctx->hub_err);
+        CK(cudaGetLastError());
+    }
     const size_t smem = (size_t)(n + 1) * sizeof(int);
     CK(cudaFuncSetAttribute(k_profit<W16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_profit<W16>, 512, smem));
     if (per_sm < 1) { set_err(ctx, "profit kernel does not fit (n=%d)", n); return BM_E_INPUT; }
     CK(cudaEventRecord(ctx->ev[4], ctx->st));
-    k_profit<W16><<<ctx->num_sms * per_sm, 512, smem, ctx->st>>>(g, ctx->order, ctx->small);
+    k_profit<W16><<<ctx->num_sms * per_sm, 512, smem, ctx->st>>>(g, ctx->order, ctx->small,
+                                                                ctx->nh ? ctx->is_hub : nullptr, kHubT);
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev[5], ctx->st));
     return BM_OK;
@@ -530,14 +550,13 @@ static bm_status stage_commit(bm_ctx* ctx, const bm_sweep_opts* o) {
     CK(cudaGetLastError());
     size_t tb = ctx->cub_bytes;
     CK(cub::DeviceRadixSort::SortKeys(ctx->cub_tmp, tb, ctx->ckeys, ctx->ckeys_sorted, n, 0, 64, ctx->st));
-    if (!ctx->pold) CK(dalloc(ctx, &ctx->pold, (size_t)(n + 1) * sizeof(int)));
     const int max_scan = o ? o->max_candidates : 0;
     const int max_verify = o ? o->max_verify : -1;
     const int lim = (max_scan > 0 && max_scan < n) ? max_scan : n;
-    const size_t smem = (size_t)n;
-    CK(cudaFuncSetAttribute(k_commit_seq<W16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_commit_seq<W16><<<1, 1024, smem, ctx->st>>>(view<W16>(ctx), ctx->ckeys_sorted, lim, max_verify, ctx->pold,
-                                                  ctx->cstats);
+    const size_t smem = commit_group_smem(n);
+    CK(cudaFuncSetAttribute(k_commit_group<W16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_commit_group<W16><<<1, 1024, smem, ctx->st>>>(view<W16>(ctx), ctx->ckeys_sorted, lim, max_verify,
+                                                    ctx->cstats);
     CK(cudaGetLastError());
     return BM_OK;
 }
@@ -593,10 +612,13 @@ extern "C" bm_status bm_sweep(bm_ctx* ctx, const bm_sweep_opts* opts, bm_sweep_s
     CommitStats cs;
     int small[3];
     unsigned long long terms = 0;
+    int herr = 0;
     CK(cudaMemcpyAsync(&cs, ctx->cstats, sizeof cs, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaMemcpyAsync(small, ctx->small, 3 * sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaMemcpyAsync(&terms, ctx->work_sum, sizeof terms, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(&herr, ctx->hub_err, sizeof herr, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
+    if (herr) { set_err(ctx, "bm_sweep: tensor-core hub GEMM wait timed out"); return BM_E_TIMEOUT; }
     ctx->score = before + cs.total_delta;
     if (stats) {
         memset(stats, 0, sizeof *stats);
@@ -608,12 +630,16 @@ extern "C" bm_status bm_sweep(bm_ctx* ctx, const bm_sweep_opts* opts, bm_sweep_s
         stats->scanned = cs.scanned;
         stats->verified = cs.verified;
         stats->committed = cs.committed;
-        cudaEventElapsedTime(&stats->ms_prep, ctx->ev[0], ctx->ev[4]);
+        cudaEventElapsedTime(&stats->ms_prep, ctx->ev[0], ctx->ev_hub);
+        cudaEventElapsedTime(&stats->ms_hub, ctx->ev_hub, ctx->ev[4]);
         cudaEventElapsedTime(&stats->ms_profit, ctx->ev[4], ctx->ev[5]);
         cudaEventElapsedTime(&stats->ms_combine, ctx->ev[1], ctx->ev[2]);
         cudaEventElapsedTime(&stats->ms_commit, ctx->ev[2], ctx->ev[3]);
         cudaEventElapsedTime(&stats->ms_total, ctx->ev[0], ctx->ev[3]);
         stats->min_terms = (long long)terms;
+        stats->commit_entries = cs.entries;
+        stats->commit_steps = cs.steps;
+        stats->commit_carried = cs.carried;
     }
     return BM_OK;
 }

@@ -1,0 +1,107 @@
+// bm_internal.cuh -- engine context shared by the single-instance and the
+// batched entry points (internal; not part of the C ABI).
+#pragma once
+#include <cstdio>
+#include <cstdarg>
+#include <cuda_runtime.h>
+#include "bm.h"
+#include "bm_kernels.cuh"
+
+using namespace bm;
+
+struct bm_ctx {
+    int n = 0;
+    bool w16 = true;
+    int dev = 0, num_sms = 0;
+    long long e1 = 0, e2 = 0, nself = 0;
+    cudaStream_t st = nullptr;
+    char err[512] = {0};
+    bool mapped = false;
+    long long score = 0;  // score of the current matching (kept exact across commits)
+    // device buffers
+    int *off1o = nullptr, *off1i = nullptr, *off2o = nullptr, *off2i = nullptr, *offs = nullptr, *selfw = nullptr;
+    void *ent1o = nullptr, *ent1i = nullptr, *ent2o = nullptr, *ent2i = nullptr;
+    void *ent1oP = nullptr, *ent1iP = nullptr, *ent2oP = nullptr, *ent2iP = nullptr;
+    int* off2oH = nullptr;                  // G2 out-entries with weight above the hub threshold
+    void *ent2oH = nullptr, *ent2oHP = nullptr;
+    long long e2H = 0;
+    void* W2 = nullptr;
+    void* W2T = nullptr;
+    int *p = nullptr, *pinv = nullptr;
+    int* S = nullptr;
+    unsigned long long* rowbest = nullptr;
+    unsigned long long *ckeys = nullptr, *ckeys_sorted = nullptr;
+    unsigned long long *wkeys = nullptr, *wkeys_sorted = nullptr;
+    int *wvals = nullptr, *order = nullptr;
+    void* cub_tmp = nullptr;
+    size_t cub_bytes = 0;
+    int* small = nullptr;          // [0]=row counter [1]=ncand [2]=best delta
+    unsigned long long* score_acc = nullptr;
+    CommitStats* cstats = nullptr;
+    int* scratch_pairs = nullptr;  // pair/triple inputs and outputs (ints)
+    long long scratch_cap = 0;
+    unsigned* adj = nullptr;       // G1 adjacency bitmap (3-cycles)
+    int adj_words = 0;
+    int* rowd = nullptr;           // reference-order row deltas
+    int* first = nullptr;          // [0] = first improving partner, [1] = copy for the host
+    long long* fi_acc = nullptr;   // [0] = delta sum, [1] = commits
+    unsigned long long* tcount = nullptr;
+    long long dev_bytes = 0;
+    cudaEvent_t ev[6] = {};
+    cudaEvent_t uev[8] = {};       // bm_timer_* slots
+    unsigned long long* work_sum = nullptr;
+    unsigned long long* part = nullptr;   // per-tile best partners (combine)
+    // tensor-core hub terms
+    int nh = 0, hubK = 0, Mpad = 0, Npad = 0;
+    bool hubA_built = false;
+    int* hubs = nullptr;
+    unsigned char* is_hub = nullptr;
+    uint8_t *hubA = nullptr, *hubB = nullptr;
+    int* hub_err = nullptr;
+    cudaEvent_t ev_hub = nullptr;
+};
+
+// Records an error message on the context (or, with c == NULL, in the
+// thread's slot read by bm_last_error(NULL)).
+void set_err(bm_ctx* c, const char* fmt, ...);
+
+#define CK(call)                                                                   \
+    do {                                                                           \
+        cudaError_t e_ = (call);                                                   \
+        if (e_ != cudaSuccess) {                                                   \
+            set_err(ctx, "%s:%d: %s: %s", __FILE__, __LINE__, #call,               \
+                    cudaGetErrorString(e_));                                       \
+            return BM_E_CUDA;                                                      \
+        }                                                                          \
+    } while (0)
+
+template <typename T>
+static cudaError_t dalloc(bm_ctx* ctx, T** ptr, size_t bytes) {
+    cudaError_t e = cudaMalloc((void**)ptr, bytes ? bytes : 16);
+    if (e == cudaSuccess) ctx->dev_bytes += (long long)bytes;
+    return e;
+}
+
+template <bool W16>
+inline DevView<W16> view(bm_ctx* c) {
+    DevView<W16> g;
+    typedef typename Ent<W16>::T E;
+    typedef typename Dense<W16>::T D;
+    g.n = c->n;
+    g.off1o = c->off1o; g.ent1o = (const E*)c->ent1o;
+    g.off1i = c->off1i; g.ent1i = (const E*)c->ent1i;
+    g.off2o = c->off2o; g.ent2o = (const E*)c->ent2o;
+    g.off2i = c->off2i; g.ent2i = (const E*)c->ent2i;
+    g.offs = c->offs; g.selfw = c->selfw;
+    g.ent1oP = (E*)c->ent1oP; g.ent1iP = (E*)c->ent1iP;
+    g.ent2oP = (E*)c->ent2oP; g.ent2iP = (E*)c->ent2iP;
+    g.off2oH = c->off2oH; g.ent2oHP = (E*)c->ent2oHP;
+    g.W2 = (const D*)c->W2;
+    g.W2T = (const D*)c->W2T;
+    g.p = c->p; g.pinv = c->pinv;
+    g.S = c->S;
+    return g;
+}
+
+// Allocates the n x n profit matrix on first use.
+bm_status ensure_S(bm_ctx* ctx);

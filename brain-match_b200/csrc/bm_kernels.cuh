@@ -60,11 +60,17 @@ template <bool W16> struct DevView {
     const int* offs;  const int* selfw; // G1 self-loops per vertex
     E* ent1oP; E* ent1iP;               // G1 lists with ids mapped through p
     E* ent2oP; E* ent2iP;               // G2 lists with ids mapped through pinv
+    const int* off2oH; E* ent2oHP;      // G2 out-entries above the hub threshold, mapped through pinv
     const D* W2;                        // dense (n+1)^2, row/col n zero
+    const D* W2T;                       // its transpose (columns of W2 read as rows)
     int* p; int* pinv;                  // n+1 entries, [n] = n
     int* S;                             // n*n profit matrix
     __device__ __forceinline__ int w2(int f, int g) const {
         return (int)W2[(size_t)f * (size_t)(n + 1) + (size_t)g];
+    }
+    // same value as w2(f, g), read from row g of the transpose
+    __device__ __forceinline__ int w2t(int f, int g) const {
+        return (int)W2T[(size_t)g * (size_t)(n + 1) + (size_t)f];
     }
 };
 
@@ -87,8 +93,9 @@ __global__ void k_relabel(const typename Ent<W16>::T* __restrict__ in,
 
 // Work estimate of a profit row: number of min terms it scatters.
 template <bool W16>
-__global__ void k_row_work(DevView<W16> g, unsigned long long* __restrict__ key,
-                           int* __restrict__ val, unsigned long long* __restrict__ total) {
+__global__ void k_row_work(DevView<W16> g, const unsigned char* __restrict__ is_hub,
+                           unsigned long long* __restrict__ key, int* __restrict__ val,
+                           unsigned long long* __restrict__ total) {
     typedef Ent<W16> EN;
     const int lane = threadIdx.x & 31;
     int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -100,6 +107,7 @@ __global__ void k_row_work(DevView<W16> g, unsigned long long* __restrict__ key,
             w += g.off2i[f + 1] - g.off2i[f];
         }
         for (int i = g.off1i[a] + lane; i < g.off1i[a + 1]; i += 32) {
+            if (is_hub && is_hub[EN::id(g.ent1i[i])]) continue;  // tensor-core term
             int f = EN::id(g.ent1iP[i]);
             w += g.off2o[f + 1] - g.off2o[f];
         }
@@ -141,92 +149,137 @@ __device__ __forceinline__ void scatter_list(int* acc, const typename Ent<W16>::
     for (; i < i1; i += step) { const E x = list[i]; atomicAdd(&acc[EN::id(x)], imin(w1, EN::w(x))); }
 }
 
+// Hub residual: terms of a hub in-edge (u,a,w1) above the threshold T that
+// the tensor-core GEMM does not cover, min(w1,w2) - T for w1 > T, over the
+// G2 out-entries of p(u) whose weight w2 is above T.
 template <bool W16>
-__global__ void __launch_bounds__(512)
-k_profit(DevView<W16> g, const int* __restrict__ order, int* __restrict__ counter) {
+__device__ __forceinline__ void scatter_residual(int* acc, const typename Ent<W16>::T* __restrict__ list,
+                                                 int i0, int i1, int w1, int thr, int first, int step) {
+    typedef Ent<W16> EN;
+    for (int i = i0 + first; i < i1; i += step) {
+        const typename EN::T x = list[i];
+        atomicAdd(&acc[EN::id(x)], imin(w1, EN::w(x)) - thr);
+    }
+}
+
+// One profit row of S (all threads of the block call it together; it ends
+// with a barrier).  acc holds n+1 ints of shared memory.
+template <bool W16>
+__device__ __forceinline__ void profit_row(const DevView<W16>& g, int a, int* acc, int2* s_long, int* s_nlong,
+                                           const unsigned char* __restrict__ is_hub, int hub_thr) {
     typedef Ent<W16> EN;
     typedef typename EN::T E;
+    const int n = g.n;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+    if (tid == 0) *s_nlong = 0;
+    if (is_hub) {  // the row starts from the tensor-core hub terms already in S
+        const int* row0 = g.S + (size_t)a * (size_t)n;
+        if ((n & 3) == 0) {
+            const int4* r4 = reinterpret_cast<const int4*>(row0);
+            int4* a4 = reinterpret_cast<int4*>(acc);
+            const int n4 = n >> 2;
+            int i = tid;
+            for (; i + 3 * (int)blockDim.x < n4; i += 4 * blockDim.x) {
+                const int4 x0 = r4[i], x1 = r4[i + blockDim.x], x2 = r4[i + 2 * blockDim.x], x3 = r4[i + 3 * blockDim.x];
+                a4[i] = x0; a4[i + blockDim.x] = x1; a4[i + 2 * blockDim.x] = x2; a4[i + 3 * blockDim.x] = x3;
+            }
+            for (; i < n4; i += blockDim.x) a4[i] = r4[i];
+        } else {
+            for (int i = tid; i < n; i += blockDim.x) acc[i] = row0[i];
+        }
+        if (tid == 0) acc[n] = 0;
+    } else {
+        for (int i = tid; i <= n; i += blockDim.x) acc[i] = 0;
+    }
+    __syncthreads();
+    // out-edges of a against G2 in-lists of p(v), then in-edges against out-lists of p(u)
+    const int so = g.off1o[a], lo = g.off1o[a + 1] - so;
+    const int si = g.off1i[a], li = g.off1i[a + 1] - si;
+    for (int j = wid; j < lo + li; j += nw) {
+        const bool out = j < lo;
+        const E ea = out ? g.ent1oP[so + j] : g.ent1iP[si + (j - lo)];
+        const int f = EN::id(ea), w1 = EN::w(ea);
+        const int* off = out ? g.off2i : g.off2o;
+        const E* list = out ? g.ent2iP : g.ent2oP;
+        const int b0 = off[f], b1 = off[f + 1];
+        if (!out && is_hub && is_hub[EN::id(g.ent1i[si + (j - lo)])]) {
+            if (w1 > hub_thr)
+                scatter_residual<W16>(acc, g.ent2oHP, g.off2oH[f], g.off2oH[f + 1], w1, hub_thr, lane, 32);
+            continue;
+        }
+        if (b1 - b0 > kLongList) {
+            int q = 0;
+            if (lane == 0) q = atomicAdd(s_nlong, 1);
+            q = __shfl_sync(0xffffffffu, q, 0);
+            if (q < kLongQueue) {
+                if (lane == 0) s_long[q] = make_int2(f, w1 | (out ? 0 : (int)0x80000000));
+                continue;
+            }
+        }
+        scatter_list<W16>(acc, list, b0, b1, w1, lane, 32);
+    }
+    __syncthreads();
+    // long lists, one at a time, by the whole block
+    const int nl = min(*s_nlong, kLongQueue);
+    for (int q = 0; q < nl; q++) {
+        const int2 e = s_long[q];
+        const bool out = e.y >= 0;
+        const int w1 = e.y & 0x7fffffff;
+        const int* off = out ? g.off2i : g.off2o;
+        const E* list = out ? g.ent2iP : g.ent2oP;
+        scatter_list<W16>(acc, list, off[e.x], off[e.x + 1], w1, tid, blockDim.x);
+    }
+    // corner corrections for every G1 edge a->b
+    {
+        const int pa = g.p[a];
+        for (int j = tid; j < lo; j += blockDim.x) {
+            const int b = EN::id(g.ent1o[so + j]);
+            const E ep = g.ent1oP[so + j];
+            const int pb = EN::id(ep), x = EN::w(ep);
+            const int c = imin(x, g.w2(pa, pb)) + imin(x, g.w2(pb, pa))
+                        - imin(x, g.w2(pa, pa)) - imin(x, g.w2(pb, pb));
+            if (c) atomicAdd(&acc[b], c);
+        }
+    }
+    // unary terms of G1 self-loops: a taking p(b) earns min(s, W2[p b][p b])
+    {
+        const int q0 = g.offs[a], q1 = g.offs[a + 1];
+        if (q1 > q0) {
+            __syncthreads();
+            for (int b = tid; b < n; b += blockDim.x) {
+                const int pb = g.p[b];
+                const int d = g.w2(pb, pb);
+                int t = 0;
+                for (int q = q0; q < q1; q++) t += imin(g.selfw[q], d);
+                acc[b] += t;
+            }
+        }
+    }
+    __syncthreads();
+    int* row = g.S + (size_t)a * (size_t)n;
+    if ((n & 3) == 0) {
+        int4* r4 = reinterpret_cast<int4*>(row);
+        const int4* a4 = reinterpret_cast<const int4*>(acc);
+        for (int i = tid; i < (n >> 2); i += blockDim.x) r4[i] = a4[i];
+    } else {
+        for (int i = tid; i < n; i += blockDim.x) row[i] = acc[i];
+    }
+    __syncthreads();
+}
+
+template <bool W16>
+__global__ void __launch_bounds__(512)
+k_profit(DevView<W16> g, const int* __restrict__ order, int* __restrict__ counter,
+         const unsigned char* __restrict__ is_hub, int hub_thr) {
     extern __shared__ int acc[];
     __shared__ int s_row, s_nlong;
     __shared__ int2 s_long[kLongQueue];  // (G2 vertex, w1 | kind << 31)
-    const int n = g.n;
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
     for (;;) {
-        if (tid == 0) { s_row = atomicAdd(counter, 1); s_nlong = 0; }
+        if (threadIdx.x == 0) s_row = atomicAdd(counter, 1);
         __syncthreads();
         const int r = s_row;
-        if (r >= n) break;
-        const int a = order[r];
-        for (int i = tid; i <= n; i += blockDim.x) acc[i] = 0;
-        __syncthreads();
-        // out-edges of a against G2 in-lists of p(v), then in-edges against out-lists of p(u)
-        const int so = g.off1o[a], lo = g.off1o[a + 1] - so;
-        const int si = g.off1i[a], li = g.off1i[a + 1] - si;
-        for (int j = wid; j < lo + li; j += nw) {
-            const bool out = j < lo;
-            const E ea = out ? g.ent1oP[so + j] : g.ent1iP[si + (j - lo)];
-            const int f = EN::id(ea), w1 = EN::w(ea);
-            const int* off = out ? g.off2i : g.off2o;
-            const E* list = out ? g.ent2iP : g.ent2oP;
-            const int b0 = off[f], b1 = off[f + 1];
-            if (b1 - b0 > kLongList) {
-                int q = 0;
-                if (lane == 0) q = atomicAdd(&s_nlong, 1);
-                q = __shfl_sync(0xffffffffu, q, 0);
-                if (q < kLongQueue) {
-                    if (lane == 0) s_long[q] = make_int2(f, w1 | (out ? 0 : (int)0x80000000));
-                    continue;
-                }
-            }
-            scatter_list<W16>(acc, list, b0, b1, w1, lane, 32);
-        }
-        __syncthreads();
-        // long lists, one at a time, by the whole CTA
-        const int nl = min(s_nlong, kLongQueue);
-        for (int q = 0; q < nl; q++) {
-            const int2 e = s_long[q];
-            const bool out = e.y >= 0;
-            const int w1 = e.y & 0x7fffffff;
-            const int* off = out ? g.off2i : g.off2o;
-            const E* list = out ? g.ent2iP : g.ent2oP;
-            scatter_list<W16>(acc, list, off[e.x], off[e.x + 1], w1, tid, blockDim.x);
-        }
-        // corner corrections for every G1 edge a->b
-        {
-            const int pa = g.p[a];
-            for (int j = tid; j < lo; j += blockDim.x) {
-                const int b = EN::id(g.ent1o[so + j]);
-                const E ep = g.ent1oP[so + j];
-                const int pb = EN::id(ep), x = EN::w(ep);
-                const int c = imin(x, g.w2(pa, pb)) + imin(x, g.w2(pb, pa))
-                            - imin(x, g.w2(pa, pa)) - imin(x, g.w2(pb, pb));
-                if (c) atomicAdd(&acc[b], c);
-            }
-        }
-        // unary terms of G1 self-loops: a taking p(b) earns min(s, W2[p b][p b])
-        {
-            const int q0 = g.offs[a], q1 = g.offs[a + 1];
-            if (q1 > q0) {
-                __syncthreads();
-                for (int b = tid; b < n; b += blockDim.x) {
-                    const int pb = g.p[b];
-                    const int d = g.w2(pb, pb);
-                    int t = 0;
-                    for (int q = q0; q < q1; q++) t += imin(g.selfw[q], d);
-                    acc[b] += t;
-                }
-            }
-        }
-        __syncthreads();
-        int* row = g.S + (size_t)a * (size_t)n;
-        if ((n & 3) == 0) {
-            int4* r4 = reinterpret_cast<int4*>(row);
-            const int4* a4 = reinterpret_cast<const int4*>(acc);
-            for (int i = tid; i < (n >> 2); i += blockDim.x) r4[i] = a4[i];
-        } else {
-            for (int i = tid; i < n; i += blockDim.x) row[i] = acc[i];
-        }
-        __syncthreads();
+        if (r >= g.n) break;
+        profit_row<W16>(g, order[r], acc, s_long, &s_nlong, is_hub, hub_thr);
     }
 }
 
@@ -244,7 +297,7 @@ __device__ __forceinline__ unsigned long long kmax(unsigned long long x, unsigne
 // two rows pick each other.  Sort key: (0x7fffffff - delta) << 32 | lo << 16 | hi
 // -> ascending order = delta desc, lo asc, hi asc.  Rows without a candidate
 // get ~0.
-__global__ void k_candidates(const unsigned long long* __restrict__ rowbest, int n,
+static __global__ void k_candidates(const unsigned long long* __restrict__ rowbest, int n,
                              unsigned long long* __restrict__ keys, int* __restrict__ ncand,
                              int* __restrict__ best_delta) {
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
@@ -363,7 +416,9 @@ __global__ void k_score(DevView<W16> g, unsigned long long* __restrict__ out) {
 // Counters reported by the commit kernels.
 struct CommitStats {
     long long total_delta;
-    int scanned, verified, committed, pad;
+    int scanned, verified, committed, steps;
+    long long entries;
+    int carried, pad;
 };
 
 }  // namespace bm

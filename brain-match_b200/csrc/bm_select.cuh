@@ -6,9 +6,9 @@
 //   vertex of the tile, its best partner inside the tile to a partial array
 //   P[tile column][vertex]; k_best_reduce folds the partials into rowbest.
 //   No atomics; every (tile, vertex) slot is written exactly once.
-// k_commit_seq: the sequential set commit (candidates sorted by delta desc,
+// k_commit_group: the sequential set commit (candidates sorted by delta desc,
 //   skip a pair whose vertex already moved, re-evaluate it on the current
-//   matching, commit iff > 0).
+//   matching, commit iff > 0), several pairs per step.
 #pragma once
 #include "bm_kernels.cuh"
 
@@ -16,50 +16,47 @@ namespace bm {
 
 constexpr int kTile = 64;
 
-__global__ void __launch_bounds__(256)
-k_combine64(const int* __restrict__ S, int n, unsigned long long* __restrict__ part,
-            int* __restrict__ all_out) {
-    __shared__ int sA[kTile][kTile + 1];  // sA[r][c] = S[a0+r][b0+c]
-    __shared__ int sB[kTile][kTile + 1];  // sB[r][c] = S[b0+r][a0+c]
-    __shared__ int dA[kTile], dB[kTile];
-    __shared__ unsigned long long cpart[8][kTile];
-    const int ti = blockIdx.y, tj = blockIdx.x;
-    if (ti > tj) return;
-    const int a0 = ti * kTile, b0 = tj * kTile;
+// One TxT tile (ti <= tj) of the upper triangle, 256 threads (T = 32 or 64).
+template <int T>
+__device__ __forceinline__ void combine_tile(const int* __restrict__ S, int n, int ti, int tj,
+                                             unsigned long long* __restrict__ part, int* __restrict__ all_out) {
+    constexpr int CL = T / 32;            // columns per lane
+    __shared__ int sA[T][T + 1];          // sA[r][c] = S[a0+r][b0+c]
+    __shared__ int sB[T][T + 1];          // sB[r][c] = S[b0+r][a0+c]
+    __shared__ int dA[T], dB[T];
+    __shared__ unsigned long long cpart[8][T];
+    const int a0 = ti * T, b0 = tj * T;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;  // 8 warps
-    for (int i = tid; i < kTile * kTile; i += 256) {
-        const int r = i >> 6, c = i & 63;
+    for (int i = tid; i < T * T; i += 256) {
+        const int r = i / T, c = i % T;
         const int a = a0 + r, b = b0 + c;
         sA[r][c] = (a < n && b < n) ? S[(size_t)a * n + b] : 0;
         const int bb = b0 + r, aa = a0 + c;
         sB[r][c] = (bb < n && aa < n) ? S[(size_t)bb * n + aa] : 0;
     }
-    if (tid < kTile) {
+    if (tid < T) {
         const int a = a0 + tid, b = b0 + tid;
         dA[tid] = a < n ? S[(size_t)a * n + a] : 0;
         dB[tid] = b < n ? S[(size_t)b * n + b] : 0;
     }
     __syncthreads();
     const bool diag = (ti == tj);
-    // columns handled by this lane: c0 = lane, c1 = lane + 32; rows r = wid, wid+8, ...
-    unsigned long long cb0 = 0, cb1 = 0;
-    const int c0 = lane, c1 = lane + 32;
-    const int b_0 = b0 + c0, b_1 = b0 + c1;
-    for (int r = wid; r < kTile; r += 8) {
+    unsigned long long cb[CL];
+#pragma unroll
+    for (int q = 0; q < CL; q++) cb[q] = 0;
+    for (int r = wid; r < T; r += 8) {
         const int a = a0 + r;
         unsigned long long rb = 0;
         if (a < n) {
-            if (b_0 < n && b_0 != a) {
-                const int d = sA[r][c0] + sB[c0][r] - dA[r] - dB[c0];
-                rb = kmax(rb, pack_best(d, b_0));
-                cb0 = kmax(cb0, pack_best(d, a));
-                if (all_out && a < b_0) all_out[(long long)a * (2LL * n - a - 1) / 2 + (b_0 - a - 1)] = d;
-            }
-            if (b_1 < n && b_1 != a) {
-                const int d = sA[r][c1] + sB[c1][r] - dA[r] - dB[c1];
-                rb = kmax(rb, pack_best(d, b_1));
-                cb1 = kmax(cb1, pack_best(d, a));
-                if (all_out && a < b_1) all_out[(long long)a * (2LL * n - a - 1) / 2 + (b_1 - a - 1)] = d;
+#pragma unroll
+            for (int q = 0; q < CL; q++) {
+                const int c = lane + 32 * q, b = b0 + c;
+                if (b < n && b != a) {
+                    const int d = sA[r][c] + sB[c][r] - dA[r] - dB[c];
+                    rb = kmax(rb, pack_best(d, b));
+                    cb[q] = kmax(cb[q], pack_best(d, a));
+                    if (all_out && a < b) all_out[(long long)a * (2LL * n - a - 1) / 2 + (b - a - 1)] = d;
+                }
             }
         }
         for (int o = 16; o; o >>= 1) rb = kmax(rb, __shfl_xor_sync(0xffffffffu, rb, o));
@@ -68,10 +65,10 @@ k_combine64(const int* __restrict__ S, int n, unsigned long long* __restrict__ p
     // column partials (vertices b of the tile, over this tile's rows); a
     // diagonal tile's row partials already cover both orders of every pair
     if (!diag) {
-        cpart[wid][c0] = cb0;
-        cpart[wid][c1] = cb1;
+#pragma unroll
+        for (int q = 0; q < CL; q++) cpart[wid][lane + 32 * q] = cb[q];
         __syncthreads();
-        if (tid < kTile) {
+        if (tid < T) {
             unsigned long long k = cpart[0][tid];
             for (int w = 1; w < 8; w++) k = kmax(k, cpart[w][tid]);
             const int b = b0 + tid;
@@ -80,8 +77,16 @@ k_combine64(const int* __restrict__ S, int n, unsigned long long* __restrict__ p
     }
 }
 
+static __global__ void __launch_bounds__(256)
+k_combine64(const int* __restrict__ S, int n, unsigned long long* __restrict__ part,
+            int* __restrict__ all_out) {
+    const int ti = blockIdx.y, tj = blockIdx.x;
+    if (ti > tj) return;
+    combine_tile<kTile>(S, n, ti, tj, part, all_out);
+}
+
 // rowbest[x] = max over tile columns t of part[t][x]
-__global__ void k_best_reduce(const unsigned long long* __restrict__ part, int n, int tiles,
+static __global__ void k_best_reduce(const unsigned long long* __restrict__ part, int n, int tiles,
                               unsigned long long* __restrict__ rowbest) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     if (x >= n) return;
@@ -91,38 +96,68 @@ __global__ void k_best_reduce(const unsigned long long* __restrict__ part, int n
 }
 
 // ---------------------------------------------------------------------------
-// Sequential set commit (one CTA), candidates in sorted order:
+// Set commit (one CTA).  The rule is sequential over the sorted candidates:
 //   * skip the pair if either vertex already moved in this sweep;
 //   * otherwise its current delta is the sweep delta plus, for every G1 edge
 //     from one of its vertices x to an already-moved vertex z, the change of
-//     that edge's term between z's pre-move image (pold) and its image now.
-//     The CTA finds those edges in one coalesced pass over the pair's four
-//     edge lists (a flag check per entry; W2 is read only for moved
-//     neighbours).  A pair with at least one moved neighbour is the
-//     "re-verified" case of the rule (counted, and limited by max_verify);
+//     that edge's term between z's pre-move image (pold) and its image now;
+//     a pair with at least one moved neighbour is the "re-verified" case
+//     (counted, and limited by max_verify);
 //   * commit iff the current delta is > 0.
-// Warp 0 skips runs of candidates with a moved vertex 32 at a time, so only
-// live candidates cost a pass of the CTA.
+// It is executed kCG pairs at a time: the CTA makes one coalesced pass over
+// the step's edge lists (entries spread evenly over all threads, so a hub
+// pair does not stall the step), accumulating each pair's correction
+// from moved neighbours (a flag check per entry; W2 is read only for moved
+// neighbours) and noting which earlier pairs of the step it shares a vertex
+// with or is G1-adjacent to.  Thread 0 then decides the pairs in order; a pair
+// that touches an earlier pair of the step that committed or is still
+// undecided is carried, in order, into the next step and scanned again.  A
+// pair's delta depends only on p at its vertices and their G1 neighbours, so
+// every decision equals the one-at-a-time rule's.  With a re-verification
+// budget the step stops at the first carried pair, so the budget is spent in
+// the sequential order.
+constexpr int kCG = 8;                 // pairs per step
+
+// 16-bit atomic OR in shared memory through the aligned 32-bit word.
+__device__ __forceinline__ void atomicOr_u16(uint16_t* p, uint16_t v) {
+    const size_t addr = reinterpret_cast<size_t>(p);
+    unsigned* w = reinterpret_cast<unsigned*>(addr & ~(size_t)3);
+    atomicOr(w, (unsigned)v << ((addr & 2) ? 16 : 0));
+}
+
+// The set commit of one instance; all 1024 threads of the block call it.
+// smem: commit_group_smem(n) bytes of dynamic shared memory.
 template <bool W16>
-__global__ void __launch_bounds__(1024)
-k_commit_seq(DevView<W16> g, const unsigned long long* __restrict__ keys, int lim, int max_verify,
-             int* __restrict__ pold, CommitStats* __restrict__ st) {
+__device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsigned long long* __restrict__ keys,
+                                             int lim, int max_verify, CommitStats* __restrict__ st,
+                                             unsigned char* smem) {
     typedef Ent<W16> EN;
-    extern __shared__ unsigned char used[];  // n bytes
-    __shared__ int s_k, s_lo, s_hi, s_d0, s_done, s_scanned;
-    __shared__ int s_red[32], s_cnt[32];
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nwarp = blockDim.x >> 5;
+    // shared: used[n] flags, then the matching and the pre-move images as
+    // 16-bit ids (n <= 65535, so the "unmatched" value n fits)
     const int n = g.n;
-    for (int i = tid; i < n; i += blockDim.x) used[i] = 0;
-    if (tid == 0) { s_k = 0; s_scanned = 0; }
-    long long total = 0;
-    int verified = 0, committed = 0;
+    unsigned char* used = smem;
+    uint16_t* p16 = reinterpret_cast<uint16_t*>(smem + ((n + 15) & ~15));
+    uint16_t* q16 = p16 + ((n + 8) & ~7);
+    uint16_t* mark = q16 + ((n + 8) & ~7);  // bit i set: vertex belongs to pair i of the step
+    __shared__ int s_lo[kCG], s_hi[kCG], s_d0[kCG];
+    __shared__ int s_corr[kCG], s_cnt[kCG], s_pre[kCG + 1];
+    __shared__ unsigned s_imask[kCG];   // earlier pairs of the step G1-adjacent to this one
+    __shared__ unsigned s_share[kCG];   // earlier pairs of the step sharing a vertex with this one
+    __shared__ unsigned s_dead;         // pairs with a vertex already moved when the step starts
+    __shared__ int s_inf[kCG][7];       // la0, la, ia0, ia, lb0, lb, ib0
+    __shared__ int s_n, s_k, s_scanned;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    for (int i = tid; i < n; i += blockDim.x) { used[i] = 0; p16[i] = (uint16_t)g.p[i]; mark[i] = 0; }
+    if (tid == 0) { s_n = 0; s_k = 0; s_scanned = 0; p16[n] = (uint16_t)n; }
+    long long total = 0, entries = 0;
+    int verified = 0, committed = 0, steps = 0, carried = 0;
     __syncthreads();
     for (;;) {
-        // ---- warp 0: next candidate whose vertices have not moved ----
+        // ---- warp 0: append live candidates after the carried ones, then the
+        //      per-pair list extents and their prefix (lane j = pair j) ----
         if (wid == 0) {
-            int k = s_k, scanned = s_scanned, done = 1;
-            while (k < lim) {
+            int cnt = s_n, k = s_k, scanned = s_scanned;
+            while (cnt < kCG && k < lim) {
                 const int idx = k + lane;
                 const unsigned long long key = idx < lim ? keys[idx] : ~0ull;
                 const bool valid = key != ~0ull;
@@ -131,88 +166,193 @@ k_commit_seq(DevView<W16> g, const unsigned long long* __restrict__ keys, int li
                 const bool live = valid && !used[lo] && !used[hi];
                 const unsigned vmask = __ballot_sync(0xffffffffu, valid);
                 const unsigned lmask = __ballot_sync(0xffffffffu, live);
-                if (lmask) {
-                    const int l = __ffs(lmask) - 1;
-                    scanned += l + 1;
-                    if (lane == l) {
-                        s_lo = lo; s_hi = hi;
-                        s_d0 = (int)(0x7fffffffu - (unsigned)(key >> 32));
-                    }
-                    k += l + 1;
-                    done = 0;
-                    break;
-                }
+                const int room = kCG - cnt;
+                const int before = __popc(lmask & ((1u << lane) - 1u));
                 const int nvalid = __popc(vmask);  // valid keys form a prefix
-                scanned += nvalid;
-                k += 32;
-                if (nvalid < 32) { k = lim; break; }
+                int consumed = nvalid, took = __popc(lmask);
+                if (took > room) {  // stop just before the (room+1)-th live candidate
+                    const unsigned over = __ballot_sync(0xffffffffu, live && before == room);
+                    consumed = __ffs(over) - 1;
+                    took = room;
+                }
+                if (live && before < room) {
+                    s_lo[cnt + before] = lo; s_hi[cnt + before] = hi;
+                    s_d0[cnt + before] = (int)(0x7fffffffu - (unsigned)(key >> 32));
+                }
+                cnt += took;
+                k += consumed;
+                scanned += consumed;
+                if (consumed == nvalid && nvalid < 32) { k = lim; break; }
             }
-            if (lane == 0) { s_k = k; s_scanned = scanned; s_done = done; }
+            __syncwarp();
+            int len = 0;
+            if (lane < cnt) {
+                const int a = s_lo[lane], b = s_hi[lane];
+                const int la0 = g.off1o[a], la = g.off1o[a + 1] - la0;
+                const int ia0 = g.off1i[a], ia = g.off1i[a + 1] - ia0;
+                const int lb0 = g.off1o[b], lb = g.off1o[b + 1] - lb0;
+                const int ib0 = g.off1i[b], ib = g.off1i[b + 1] - ib0;
+                s_inf[lane][0] = la0; s_inf[lane][1] = la; s_inf[lane][2] = ia0; s_inf[lane][3] = ia;
+                s_inf[lane][4] = lb0; s_inf[lane][5] = lb; s_inf[lane][6] = ib0;
+                len = la + ia + lb + ib;
+                s_corr[lane] = 0; s_cnt[lane] = 0; s_imask[lane] = 0;
+                atomicOr_u16(&mark[a], (uint16_t)(1u << lane));
+                atomicOr_u16(&mark[b], (uint16_t)(1u << lane));
+                unsigned sh = 0;
+                for (int i = 0; i < lane; i++)
+                    if (a == s_lo[i] || a == s_hi[i] || b == s_lo[i] || b == s_hi[i]) sh |= 1u << i;
+                s_share[lane] = sh;
+            }
+            int incl = len;  // inclusive prefix over lanes
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            if (lane < cnt) s_pre[lane + 1] = incl;
+            const unsigned dead = __ballot_sync(0xffffffffu, lane < cnt && (used[s_lo[lane < cnt ? lane : 0]] | used[s_hi[lane < cnt ? lane : 0]]));
+            if (lane == 0) {
+                s_pre[0] = 0; s_dead = dead;
+                s_n = cnt; s_k = k; s_scanned = scanned;
+            }
+            if (cnt) {
+                const int tot = __shfl_sync(0xffffffffu, incl, cnt - 1);
+                if (lane == 0) { entries += tot; steps++; }
+            }
         }
         __syncthreads();
-        if (s_done) break;
-        const int a = s_lo, b = s_hi;
-        // ---- corrections from edges to already-moved vertices ----
-        int corr = 0, cnt = 0;
+        const int cnt = s_n;
+        if (cnt == 0) break;
+        // ---- scan all pairs of the step, entries spread over the CTA; each
+        //      thread resolves kMLP entries and issues their loads together ----
         {
-            const int pa = g.p[a], pb = g.p[b];
-            const int la0 = g.off1o[a], la = g.off1o[a + 1] - la0;
-            const int ia0 = g.off1i[a], ia = g.off1i[a + 1] - ia0;
-            const int lb0 = g.off1o[b], lb = g.off1o[b + 1] - lb0;
-            const int ib0 = g.off1i[b], ib = g.off1i[b + 1] - ib0;
-            const int tot = la + ia + lb + ib;
-            for (int e = tid; e < tot; e += blockDim.x) {
-                int q = e, kind;
-                typename EN::T en;
-                if (q < la) { en = g.ent1o[la0 + q]; kind = 0; }
-                else if ((q -= la) < ia) { en = g.ent1i[ia0 + q]; kind = 1; }
-                else if ((q -= ia) < lb) { en = g.ent1o[lb0 + q]; kind = 2; }
-                else { q -= lb; en = g.ent1i[ib0 + q]; kind = 3; }
-                const int x = EN::id(en);
-                if (x == a || x == b || !used[x]) continue;
-                const int w = EN::w(en), px = g.p[x], qx = pold[x];
-                if (kind == 0)      corr += (imin(w, g.w2(pb, px)) - imin(w, g.w2(pa, px))) - (imin(w, g.w2(pb, qx)) - imin(w, g.w2(pa, qx)));
-                else if (kind == 1) corr += (imin(w, g.w2(px, pb)) - imin(w, g.w2(px, pa))) - (imin(w, g.w2(qx, pb)) - imin(w, g.w2(qx, pa)));
-                else if (kind == 2) corr += (imin(w, g.w2(pa, px)) - imin(w, g.w2(pb, px))) - (imin(w, g.w2(pa, qx)) - imin(w, g.w2(pb, qx)));
-                else                corr += (imin(w, g.w2(px, pa)) - imin(w, g.w2(px, pb))) - (imin(w, g.w2(qx, pa)) - imin(w, g.w2(qx, pb)));
-                cnt++;
+            constexpr int kMLP = 4;
+            const int tot = s_pre[cnt];
+            // every thread runs the same number of rounds, so warp collectives are safe
+            for (int base = 0; base < tot; base += kMLP * blockDim.x) {
+                int jj[kMLP], kind[kMLP];
+                typename EN::T en[kMLP];
+#pragma unroll
+                for (int u = 0; u < kMLP; u++) {
+                    const int e = base + tid + u * blockDim.x;
+                    jj[u] = -1;
+                    kind[u] = 0;
+                    if (e >= tot) continue;
+                    int lo = 0, hi = cnt;  // s_pre[lo] <= e < s_pre[hi]
+                    while (hi - lo > 1) { const int mid = (lo + hi) >> 1; if (s_pre[mid] <= e) lo = mid; else hi = mid; }
+                    const int j = lo;
+                    int q = e - s_pre[j];
+                    const typename EN::T* src;
+                    if (q < s_inf[j][1]) { src = g.ent1o + s_inf[j][0] + q; kind[u] = 0; }
+                    else if ((q -= s_inf[j][1]) < s_inf[j][3]) { src = g.ent1i + s_inf[j][2] + q; kind[u] = 1; }
+                    else if ((q -= s_inf[j][3]) < s_inf[j][5]) { src = g.ent1o + s_inf[j][4] + q; kind[u] = 2; }
+                    else { q -= s_inf[j][5]; src = g.ent1i + s_inf[j][6] + q; kind[u] = 3; }
+                    en[u] = *src;
+                    jj[u] = j;
+                }
+                int wv[kMLP][4];
+                bool mv[kMLP];
+#pragma unroll
+                for (int u = 0; u < kMLP; u++) {
+                    mv[u] = false;
+                    const int j = jj[u];
+                    if (j < 0) continue;
+                    const int x = EN::id(en[u]);
+                    const unsigned im = mark[x] & ((1u << j) - 1u);  // earlier pairs with vertex x
+                    if (im) atomicOr(&s_imask[j], im);
+                    const int a = s_lo[j], b = s_hi[j];
+                    if (x == a || x == b || !used[x]) continue;
+                    mv[u] = true;
+                    const int pa = p16[a], pb = p16[b], px = p16[x], qx = q16[x];
+                    if (kind[u] == 0 || kind[u] == 2) {  // out-edges of the pair's vertex: W2 rows of the images
+                        wv[u][0] = g.w2(pb, px); wv[u][1] = g.w2(pa, px); wv[u][2] = g.w2(pb, qx); wv[u][3] = g.w2(pa, qx);
+                    } else {                             // in-edges: W2 columns = rows of the transpose
+                        wv[u][0] = g.w2t(px, pb); wv[u][1] = g.w2t(px, pa); wv[u][2] = g.w2t(qx, pb); wv[u][3] = g.w2t(qx, pa);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kMLP; u++) {
+                    if (!mv[u]) continue;
+                    const int w = EN::w(en[u]);
+                    // a takes p(b) and b takes p(a): the terms of b's edges have the opposite sign
+                    int c = (imin(w, wv[u][0]) - imin(w, wv[u][1])) - (imin(w, wv[u][2]) - imin(w, wv[u][3]));
+                    if (kind[u] >= 2) c = -c;
+                    if (c) atomicAdd(&s_corr[jj[u]], c);
+                    atomicAdd(&s_cnt[jj[u]], 1);
+                }
             }
         }
-        for (int o = 16; o; o >>= 1) {
-            corr += __shfl_xor_sync(0xffffffffu, corr, o);
-            cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-        }
-        if (lane == 0) { s_red[wid] = corr; s_cnt[wid] = cnt; }
+        const int my_lo = tid < cnt ? s_lo[tid] : 0, my_hi = tid < cnt ? s_hi[tid] : 0;
         __syncthreads();
-        // ---- decide (thread 0) ----
+        // ---- clear the step's marks; decide in order (thread 0): register bitmask logic ----
+        if (tid < cnt) { mark[my_lo] = 0; mark[my_hi] = 0; }
         if (tid == 0) {
-            int c = 0, m = 0;
-            for (int w = 0; w < nwarp; w++) { c += s_red[w]; m += s_cnt[w]; }
-            bool ok = true;
-            int d = s_d0;
-            if (m > 0) {
-                if (max_verify >= 0 && verified >= max_verify) ok = false;
-                else { verified++; d += c; }
+            unsigned cm = 0, pm = 0;
+            int np = 0;
+            bool stop = false;
+            const unsigned dead = s_dead;
+            for (int j = 0; j < cnt; j++) {
+                const unsigned share = s_share[j], touch = s_imask[j] | share;
+                const bool is_dead = ((dead >> j) & 1u) || (share & cm);  // a vertex already moved
+                bool carry = stop;
+                if (!carry) {
+                    if (is_dead) continue;  // decided: skip
+                    if (touch & (cm | pm)) carry = true;
+                }
+                const int a = s_lo[j], b = s_hi[j];
+                if (carry) {
+                    if (max_verify >= 0) stop = true;
+                    carried++;
+                    pm |= 1u << j;
+                    s_lo[np] = a; s_hi[np] = b; s_d0[np] = s_d0[j];
+                    np++;
+                    continue;
+                }
+                const int moved = s_cnt[j];
+                int d = s_d0[j];
+                bool ok = true;
+                if (moved > 0) {
+                    if (max_verify >= 0 && verified >= max_verify) ok = false;
+                    else { verified++; d += s_corr[j]; }
+                }
+                if (ok && d > 0) {
+                    const int fa = p16[a], fb = p16[b];
+                    q16[a] = (uint16_t)fa; q16[b] = (uint16_t)fb;
+                    p16[a] = (uint16_t)fb; p16[b] = (uint16_t)fa;
+                    if (fb < n) g.pinv[fb] = a;
+                    if (fa < n) g.pinv[fa] = b;
+                    used[a] = 1; used[b] = 1;
+                    cm |= 1u << j;
+                    total += d;
+                    committed++;
+                }
             }
-            if (ok && d > 0) {
-                const int fa = g.p[a], fb = g.p[b];
-                pold[a] = fa; pold[b] = fb;
-                g.p[a] = fb; g.p[b] = fa;
-                if (fb < n) g.pinv[fb] = a;
-                if (fa < n) g.pinv[fa] = b;
-                used[a] = 1; used[b] = 1;
-                total += d;
-                committed++;
-            }
+            s_n = np;
         }
         __syncthreads();
     }
+    for (int i = tid; i < n; i += blockDim.x) g.p[i] = p16[i];
     if (tid == 0) {
         st->total_delta = total;
         st->scanned = s_scanned;
         st->verified = verified;
         st->committed = committed;
+        st->steps = steps;
+        st->entries = entries;
+        st->carried = carried;
     }
+}
+
+// Shared memory bytes of commit_group for n vertices.
+__host__ __device__ inline size_t commit_group_smem(int n) {
+    return (size_t)((n + 15) & ~15) + 3 * sizeof(uint16_t) * (size_t)((n + 8) & ~7);
+}
+
+template <bool W16>
+__global__ void __launch_bounds__(1024)
+k_commit_group(DevView<W16> g, const unsigned long long* __restrict__ keys, int lim, int max_verify,
+               CommitStats* __restrict__ st) {
+    extern __shared__ unsigned char smem[];
+    commit_group<W16>(g, keys, lim, max_verify, st, smem);
 }
 
 }  // namespace bm

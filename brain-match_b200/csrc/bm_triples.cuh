@@ -324,7 +324,7 @@ __global__ void k_row_first(DevView<W16> g, int m1, int start, int* __restrict__
 }
 
 // Applies the swap (m1, *first) when *first < n and records its delta.
-__global__ void k_apply_first(int* p, int* pinv, int n, int m1, const int* __restrict__ first,
+static __global__ void k_apply_first(int* p, int* pinv, int n, int m1, const int* __restrict__ first,
                               const int* __restrict__ row_d, long long* __restrict__ acc) {
     const int m2 = *first;
     if (m2 >= n) return;

@@ -49,7 +49,8 @@ typedef int32_t bm_status;
 #define BM_E_IO       -7   /* file could not be opened / written               */
 
 /* Flags for bm_create. */
-#define BM_FLAG_FORCE_I32  0x1u  /* int32 entries even when 16-bit ones fit */
+#define BM_FLAG_FORCE_I32   0x1u  /* int32 entries even when 16-bit ones fit        */
+#define BM_FLAG_NO_HUB_GEMM 0x2u  /* no tensor-core hub term (all terms scattered)   */
 
 typedef struct bm_ctx bm_ctx;
 
@@ -85,6 +86,8 @@ typedef struct {
     int64_t device_bytes;    /* device memory held by the context          */
     int32_t device;          /* CUDA ordinal                               */
     int32_t num_sms;
+    int32_t hubs;            /* G1 hubs whose in-edge terms use the tensor cores */
+    int32_t hub_k;           /* GEMM depth (hubs x thresholds), 0 if none  */
 } bm_info;
 bm_status bm_get_info(const bm_ctx* ctx, bm_info* info);
 
@@ -182,8 +185,11 @@ typedef struct {
     float   ms_commit;          /* candidate sort + sequential commit     */
     float   ms_total;           /* whole sweep                            */
     float   ms_prep;            /* relabelling + row scheduling           */
-    int32_t pad;
+    float   ms_hub;             /* hub operands + tensor-core GEMM        */
     int64_t min_terms;          /* nonzero min terms scattered            */
+    int64_t commit_entries;     /* edge-list entries read by the commit   */
+    int32_t commit_steps;       /* commit steps (pairs decided per step)  */
+    int32_t commit_carried;     /* pairs carried into a later step        */
 } bm_sweep_stats;
 
 /*
@@ -268,6 +274,49 @@ typedef struct {
  * src/triple.cu:1074-1157 (which visits only a few batches per pass).
  */
 bm_status bm_triple_round(bm_ctx* ctx, const bm_triple_opts* opts, bm_triple_stats* stats);
+
+/* ---- Batches of independent instances ---- */
+
+/*
+ * Many independent graph pairs of uneven size swept together: every
+ * instance keeps the single-instance semantics (bm_create, bm_sweep), and a
+ * batch sweep runs all of them in one set of launches -- one persistent
+ * profit-row launch over every (instance, row), one combine launch over
+ * every (instance, tile), one commit launch with a CTA per instance --
+ * captured once as a CUDA graph and replayed.  The reference runs
+ * independent instances as separate processes (MPI replicas,
+ * src/mpi-omp.c:76-122) each with the sweep of
+ * src/graph-re-alignment-gpu.cu:845-891.  The tensor-core hub term is not
+ * used in batches.
+ */
+typedef struct bm_batch bm_batch;
+
+/* Instance i has n[i] vertices and the edge arrays src1[i][0..e1[i]) etc. */
+bm_status bm_batch_create(bm_batch** out, int32_t count, const int32_t* n,
+                          const int64_t* e1, const int32_t* const* src1, const int32_t* const* dst1,
+                          const int32_t* const* w1,
+                          const int64_t* e2, const int32_t* const* src2, const int32_t* const* dst2,
+                          const int32_t* const* w2, uint32_t flags);
+void bm_batch_destroy(bm_batch* b);
+/* Last error of the batch (b may be NULL after a failed bm_batch_create). */
+const char* bm_batch_last_error(const bm_batch* b);
+bm_status bm_batch_set_mappings(bm_batch* b, const int32_t* const* maps);
+bm_status bm_batch_get_mappings(bm_batch* b, int32_t* const* maps);
+bm_status bm_batch_scores(bm_batch* b, int64_t* scores);
+/*
+ * Times the candidate launch shapes (profit-row block 256/512 threads x
+ * combine tile 32/64) on the batch itself and keeps the fastest; results
+ * never depend on the choice.
+ */
+bm_status bm_batch_autotune(bm_batch* b, int32_t* profit_threads, int32_t* combine_tile);
+/*
+ * Runs `sweeps` sweeps of every instance (graph replays).  committed (may be
+ * NULL) receives per-instance swap counts; *ms the device time.
+ */
+bm_status bm_batch_sweeps(bm_batch* b, int32_t sweeps, const bm_sweep_opts* opts, int64_t* committed,
+                          float* ms);
+bm_status bm_batch_info(const bm_batch* b, int32_t* count, int32_t* max_n, int64_t* total_pairs,
+                        int32_t* profit_threads, int32_t* combine_tile);
 
 /* ---- Host utilities: file formats and the synthetic generator ---- */
 

@@ -1,0 +1,54 @@
+"""Batched uneven instances: one set of launches (a CUDA graph per sweep) for
+all instances; every instance must end bit-identical to itself run alone."""
+import numpy as np
+import pytest
+
+import bm
+
+pytestmark = pytest.mark.gpu
+
+
+def _pairs(ns, seed0=300, **kw):
+    return [bm.generate(bm.gen_params(n=n, e=20 * n, seed=seed0 + i, **kw)) for i, n in enumerate(ns)]
+
+
+def _alone(g, sweeps, flags=bm.BM_FLAG_NO_HUB_GEMM):
+    with bm.Engine.from_pair(g, flags) as E:
+        E.set_mapping(g["map0"])
+        for _ in range(sweeps):
+            E.sweep()
+        return E.get_mapping(), E.score()
+
+
+def test_batch_sweeps_match_single_instances():
+    pairs = _pairs([300, 517, 800, 1203, 64])
+    with bm.Batch(pairs) as B:
+        B.set_mappings([g["map0"] for g in pairs])
+        info = B.info()
+        assert info["count"] == 5 and info["max_n"] == 1203
+        c1, _ = B.sweeps(2)                      # default launch shapes
+        pt, tile = B.autotune()
+        assert pt in (256, 512) and tile in (32, 64)
+        c2, ms = B.sweeps(2)                     # tuned shapes, same graph replays
+        maps, scores = B.get_mappings(), B.scores()
+    assert (c1 > 0).all()
+    for i, g in enumerate(pairs):
+        m, s = _alone(g, 4)
+        assert np.array_equal(maps[i], m), i
+        assert scores[i] == s
+
+
+def test_batch_mixed_weights_uses_one_storage_mode():
+    pairs = _pairs([400, 700])
+    big = dict(pairs[1])
+    big["w1"] = big["w1"] * 3000   # both sides reach above 16 bits
+    big["w2"] = big["w2"] * 3000
+    pairs[1] = big
+    with bm.Batch(pairs) as B:
+        B.set_mappings([g["map0"] for g in pairs])
+        B.sweeps(3)
+        maps, scores = B.get_mappings(), B.scores()
+    for i, g in enumerate(pairs):
+        m, s = _alone(g, 3, bm.BM_FLAG_NO_HUB_GEMM | bm.BM_FLAG_FORCE_I32)
+        assert np.array_equal(maps[i], m)
+        assert scores[i] == s

@@ -195,3 +195,32 @@ def test_large_weights_use_int32_path():
         E.set_mapping(m)
         assert E.score() == O.score(m)
         assert np.array_equal(E.all_deltas(), O.all_deltas(m))
+
+
+def test_hub_gemm_matches_scatter_path(cfg0):
+    """The tensor-core hub term (threshold GEMM + residual) gives the same
+    profit rows and deltas as scattering every term."""
+    g = cfg0
+    with _engine(g) as E, _engine(g, bm.BM_FLAG_NO_HUB_GEMM) as F:
+        assert E.info()["hubs"] > 0 and F.info()["hubs"] == 0
+        E.set_mapping(g["map0"])
+        F.set_mapping(g["map0"])
+        for a in (1, 2, 500, 1000):
+            assert np.array_equal(E.profit_row(a), F.profit_row(a))
+        assert np.array_equal(E.all_deltas(), F.all_deltas())
+
+
+def test_hub_gemm_heavy_weights_against_oracle():
+    """Weights far above the GEMM threshold exercise the sparse residual."""
+    g = bm.generate(bm.gen_params(n=1500, e=60000, seed=5, wmax=30000, tail_prob=0.3, geom_p=0.1))
+    O = _oracle(g)
+    m = g["map0"].copy()
+    with _engine(g) as E:
+        assert E.info()["hubs"] > 0
+        E.set_mapping(m)
+        assert np.array_equal(E.all_deltas(), O.all_deltas(m))
+        for _ in range(3):
+            E.sweep()
+            O.sweep(m)
+            assert np.array_equal(E.get_mapping(), m)
+        assert E.score() == O.score(m)

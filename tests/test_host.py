@@ -100,3 +100,17 @@ def test_create_rejects_bad_input_before_touching_the_device(bad):
         bm.Engine(n, s1, d1, w1, [1], [2], w2)
     want = bm.BM_E_OVERFLOW if bad == "overflow" else bm.BM_E_INPUT
     assert e.value.status == want
+
+
+def test_cli_argument_errors_like_the_reference(tmp_path):
+    """Usage and missing-file errors are reported before any device work."""
+    import subprocess
+    from conftest import PKG
+    binq = os.path.join(PKG, "bin", "quick")
+    bing = os.path.join(PKG, "bin", "graph-alignment-optimized")
+    r = subprocess.run([binq, "only-one-arg"], capture_output=True, text=True)
+    assert r.returncode == 1 and "Usage" in r.stderr
+    (tmp_path / "o.csv").write_text("node,order\n")
+    r = subprocess.run([bing, "gm.csv", "gf.csv", str(tmp_path / "missing.csv"), str(tmp_path / "o.csv"),
+                        "in.csv", "out.csv"], capture_output=True, text=True)
+    assert r.returncode == 1 and "Error opening file" in r.stderr
