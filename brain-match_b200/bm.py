@@ -58,6 +58,15 @@ class TripleStats(C.Structure):
                 ("ms_commit", C.c_float), ("ms_total", C.c_float)]
 
 
+class MlpTrainStats(C.Structure):
+    _fields_ = [("samples", C.c_int64), ("steps", C.c_int64), ("first_loss", C.c_float), ("last_loss", C.c_float)]
+
+
+class LearnedOpts(C.Structure):
+    _fields_ = [("pool", C.c_int32), ("per_row", C.c_int32), ("top_fraction", C.c_double), ("seed", C.c_uint64),
+                ("retries", C.c_int32), ("reserved", C.c_int32)]
+
+
 def _p(a):
     return a.ctypes.data_as(C.c_void_p)
 
@@ -104,6 +113,21 @@ def lib():
         L.bm_batch_autotune.argtypes = [vp, C.POINTER(i32), C.POINTER(i32)]
         L.bm_batch_sweeps.argtypes = [vp, i32, C.POINTER(SweepOpts), vp, C.POINTER(C.c_float)]
         L.bm_batch_info.argtypes = [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(i64), C.POINTER(i32), C.POINTER(i32)]
+        L.bm_mlp_param_count.restype = i64
+        L.bm_mlp_param_count.argtypes = []
+        L.bm_mlp_create.argtypes = [C.POINTER(vp), C.c_uint64]
+        L.bm_mlp_destroy.argtypes = [vp]
+        L.bm_mlp_destroy.restype = None
+        L.bm_mlp_last_error.restype = C.c_char_p
+        L.bm_mlp_last_error.argtypes = [vp]
+        L.bm_mlp_get_params.argtypes = [vp, vp]
+        L.bm_mlp_set_params.argtypes = [vp, vp]
+        L.bm_mlp_features.argtypes = [vp, vp, vp, vp]
+        L.bm_mlp_rank_pairs.argtypes = [vp, vp, i64, vp, vp, vp]
+        L.bm_mlp_forward.argtypes = [vp, i64, vp, vp]
+        L.bm_mlp_train_step.argtypes = [vp, i64, vp, vp, C.c_float, C.POINTER(C.c_float), vp]
+        L.bm_mlp_train_from.argtypes = [vp, vp, i32, i32, i32, C.c_float, C.c_uint64, C.POINTER(MlpTrainStats)]
+        L.bm_learned_sweep.argtypes = [vp, vp, C.POINTER(LearnedOpts), C.POINTER(SweepStats), C.POINTER(i32)]
         L.bm_free.argtypes = [vp]
         L.bm_free.restype = None
         L.bm_read_graph_csv.argtypes = [C.c_char_p, C.POINTER(i64), C.POINTER(vp), C.POINTER(vp),
@@ -383,3 +407,101 @@ class Batch:
         vals = [C.c_int32(), C.c_int32(), C.c_int64(), C.c_int32(), C.c_int32()]
         self._chk(lib().bm_batch_info(self.h, *[C.byref(v) for v in vals]))
         return dict(zip(("count", "max_n", "total_pairs", "profit_threads", "combine_tile"), [v.value for v in vals]))
+
+
+# ---- learned swap proposal ---------------------------------------------------
+MLP_IN, MLP_HID = 128, 256
+
+
+class Mlp:
+    """The proposal network (128 -> 256 -> 256 -> 1) on the current CUDA device.
+
+    Parameters are fp32 in the order W1[256][128], b1[256], W2[256][256],
+    b2[256], w3[256], b3 (bm_mlp_param_count() values)."""
+
+    def __init__(self, seed=0):
+        h = C.c_void_p()
+        st = lib().bm_mlp_create(C.byref(h), int(seed))
+        if st != BM_OK:
+            raise BMError(st, (lib().bm_mlp_last_error(None) or b"").decode())
+        self.h = h
+        self.count = int(lib().bm_mlp_param_count())
+
+    def _chk(self, st):
+        if st != BM_OK:
+            raise BMError(st, (lib().bm_mlp_last_error(self.h) or b"").decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().bm_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def get_params(self):
+        out = np.zeros(self.count, np.float32)
+        self._chk(lib().bm_mlp_get_params(self.h, _p(out)))
+        return out
+
+    def set_params(self, params):
+        params = np.ascontiguousarray(params, np.float32)
+        assert params.size == self.count
+        self._chk(lib().bm_mlp_set_params(self.h, _p(params)))
+
+    def features(self, engine):
+        """(F1, F2): per-vertex features of engine's graphs and current matching."""
+        f1 = np.zeros((engine.n, 32), np.float32)
+        f2 = np.zeros((engine.n, 32), np.float32)
+        self._chk(lib().bm_mlp_features(self.h, engine.h, _p(f1), _p(f2)))
+        return f1, f2
+
+    def rank_pairs(self, engine, m1, m2):
+        """Network scores of the 1-based pairs (m1[i], m2[i]) on engine's matching."""
+        a = np.ascontiguousarray(m1, np.int32)
+        b = np.ascontiguousarray(m2, np.int32)
+        out = np.zeros(len(a), np.float32)
+        self._chk(lib().bm_mlp_rank_pairs(self.h, engine.h, len(a), _p(a), _p(b), _p(out)))
+        return out
+
+    def forward(self, x):
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, MLP_IN)
+        out = np.zeros(len(x), np.float32)
+        self._chk(lib().bm_mlp_forward(self.h, len(x), _p(x), _p(out)))
+        return out
+
+    def train_step(self, x, target, lr=0.0, want_grads=True):
+        """One forward/backward pass; returns (loss, grads or None)."""
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, MLP_IN)
+        t = np.ascontiguousarray(target, np.float32)
+        assert len(t) == len(x)
+        loss = C.c_float()
+        g = np.zeros(self.count, np.float32) if want_grads else None
+        self._chk(lib().bm_mlp_train_step(self.h, len(x), _p(x), _p(t), float(lr), C.byref(loss),
+                                          _p(g) if want_grads else None))
+        return loss.value, g
+
+    def train_from(self, engine, sweeps=2, extra_partners=16, epochs=1, lr=1e-2, seed=0):
+        st = MlpTrainStats()
+        self._chk(lib().bm_mlp_train_from(self.h, engine.h, int(sweeps), int(extra_partners), int(epochs),
+                                          float(lr), int(seed), C.byref(st)))
+        return dict(samples=st.samples, steps=st.steps, first_loss=st.first_loss, last_loss=st.last_loss)
+
+    def learned_sweep(self, engine, pool=64, top_fraction=0.02, seed=0, per_row=0, retries=0):
+        """One learned sweep of engine's matching; returns its stats with 'fell_back'."""
+        o = LearnedOpts(int(pool), int(per_row), float(top_fraction), int(seed), int(retries), 0)
+        s = SweepStats()
+        fb = C.c_int32()
+        self._chk(lib().bm_learned_sweep(engine.h, self.h, C.byref(o), C.byref(s), C.byref(fb)))
+        d = {k: getattr(s, k) for k, _ in SweepStats._fields_ if k != "reserved"}
+        d["fell_back"] = fb.value
+        return d

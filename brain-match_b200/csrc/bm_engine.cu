@@ -8,6 +8,7 @@
 #include <cstring>
 #include <cstdarg>
 #include <vector>
+#include <atomic>
 #include <algorithm>
 #include <utility>
 #include <mutex>
@@ -222,7 +223,9 @@ extern "C" bm_status bm_create(bm_ctx** out, int32_t n, int64_t e1, const int32_
         for (auto& x : gs.w) x = std::min(x, clamp1);
     }
 
+    static std::atomic<unsigned long long> next_serial{1};
     bm_ctx* ctx = new (std::nothrow) bm_ctx();
+    if (ctx) ctx->serial = next_serial.fetch_add(1);
     if (!ctx) { set_err(nullptr, "bm_create: out of host memory"); return BM_E_NOMEM; }
     ctx->n = n;
     ctx->w16 = w16;
@@ -465,7 +468,7 @@ bm_status ensure_S(bm_ctx* ctx) {
 }
 
 template <bool W16>
-static bm_status stage_profit(bm_ctx* ctx) {
+bm_status stage_profit(bm_ctx* ctx) {
     typedef typename Ent<W16>::T E;
     DevView<W16> g = view<W16>(ctx);
     const int n = ctx->n;
@@ -516,7 +519,10 @@ static bm_status stage_profit(bm_ctx* ctx) {
     return BM_OK;
 }
 
-static bm_status stage_combine(bm_ctx* ctx, int* all_out) {
+template bm_status stage_profit<true>(bm_ctx*);
+template bm_status stage_profit<false>(bm_ctx*);
+
+bm_status stage_combine(bm_ctx* ctx, int* all_out) {
     const int n = ctx->n;
     const int t = (n + kTile - 1) / kTile;
     if (!ctx->part) CK(dalloc(ctx, &ctx->part, (size_t)t * n * sizeof(unsigned long long)));

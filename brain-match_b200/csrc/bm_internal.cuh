@@ -18,6 +18,7 @@ struct bm_ctx {
     char err[512] = {0};
     bool mapped = false;
     long long score = 0;  // score of the current matching (kept exact across commits)
+    unsigned long long serial = 0;  // unique per context in the process (caches keyed on a context)
     // device buffers
     int *off1o = nullptr, *off1i = nullptr, *off2o = nullptr, *off2i = nullptr, *offs = nullptr, *selfw = nullptr;
     void *ent1o = nullptr, *ent1i = nullptr, *ent2o = nullptr, *ent2i = nullptr;
@@ -105,3 +106,7 @@ inline DevView<W16> view(bm_ctx* c) {
 
 // Allocates the n x n profit matrix on first use.
 bm_status ensure_S(bm_ctx* ctx);
+// Sweep stages shared by the exhaustive and the learned sweep (bm_engine.cu):
+// the profit matrix S of the current matching, then each row's best partner.
+template <bool W16> bm_status stage_profit(bm_ctx* ctx);
+bm_status stage_combine(bm_ctx* ctx, int* all_out);

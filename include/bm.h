@@ -318,6 +318,110 @@ bm_status bm_batch_sweeps(bm_batch* b, int32_t sweeps, const bm_sweep_opts* opts
 bm_status bm_batch_info(const bm_batch* b, int32_t* count, int32_t* max_n, int64_t* total_pairs,
                         int32_t* profit_threads, int32_t* combine_tile);
 
+/* ---- Learned swap proposal ----
+ *
+ * A small network ranks candidate swaps so that only the top-ranked ones are
+ * evaluated exactly; the exact integer delta (bm_pair_deltas' arithmetic)
+ * judges every move and the engine's set commit applies them, so scores stay
+ * exact whatever the network says.  The reference has no learned component;
+ * its exhaustive sweep (src/graph-re-alignment-gpu.cu:845-891) is the
+ * fallback.
+ *
+ * Network: 128 -> 256 -> 256 -> 1, ReLU, bf16 weights and activations with
+ * fp32 accumulation on the tensor cores, fp32 master weights, plain SGD on the
+ * mean squared error.  Input of a pair (a, b) with images p(a), p(b):
+ * [f1(a), f1(b), f2(p(a)), f2(p(b))], 32 features per vertex (see
+ * bm_mlp_features).  Target: sign(d) log1p|d| of the exact delta d.
+ *
+ * Parameter layout (fp32, bm_mlp_param_count() values): W1[256][128], b1[256],
+ * W2[256][256], b2[256], w3[256], b3.  Layer l computes
+ * h_l = relu(W_l h_{l-1} + b_l); y = w3 . h2 + b3.
+ */
+typedef struct bm_mlp bm_mlp;
+
+typedef struct {
+    int64_t samples;    /* training rows seen (over epochs)        */
+    int64_t steps;      /* SGD steps (batches of 1024 rows)        */
+    float first_loss;   /* mean batch loss over the first epoch    */
+    float last_loss;    /* mean batch loss over the last epoch     */
+} bm_mlp_train_stats;
+
+typedef struct {
+    int32_t pool;          /* partners ranked per vertex (default 64)            */
+    int32_t per_row;       /* > 0: each vertex's per_row best-ranked partners are
+                              evaluated (n * per_row pairs; pool <= 1024,
+                              per_row <= 32); 0: the top_fraction below       */
+    double top_fraction;   /* fraction of the whole ranked pool evaluated exactly
+                              when per_row == 0 (default 0.02)                 */
+    uint64_t seed;         /* pool sampling seed                                 */
+    int32_t retries;       /* further attempts with a fresh pool before the
+                              exhaustive fallback (default 0)                  */
+    int32_t reserved;
+} bm_learned_opts;
+
+int64_t bm_mlp_param_count(void);
+/* He-uniform weights from a seeded generator, zero biases; on the current device. */
+bm_status bm_mlp_create(bm_mlp** out, uint64_t seed);
+void bm_mlp_destroy(bm_mlp* m);
+/* Last error of the network (m may be NULL after a failed bm_mlp_create). */
+const char* bm_mlp_last_error(const bm_mlp* m);
+bm_status bm_mlp_get_params(bm_mlp* m, float* params);
+bm_status bm_mlp_set_params(bm_mlp* m, const float* params);
+/*
+ * The per-vertex features of ctx's graphs under its current matching, as the
+ * network sees them: f1[a*32 + c] for G1 vertex a, f2[f*32 + c] for G2 vertex
+ * f (0-based ids).  Columns before normalisation: 0/1 out/in degree, 2/3
+ * out/in weight sums, 4/5 2-hop out/in counts, 6/7 max out/in weight, 8 G1
+ * self-loop weight, 9 current overlap contribution (G2: of the G1 vertex
+ * matched to it), all through log1p; 10 that contribution / (incident
+ * weight + 1); 11..31 zero.  Each column is then z-scored over the vertices
+ * (population std; 0 for a constant column).
+ */
+bm_status bm_mlp_features(bm_mlp* m, bm_ctx* ctx, float* f1, float* f2);
+/*
+ * Network scores of k vertex pairs (m1[i], m2[i]), 1-based, on ctx's current
+ * matching: the ranking the learned sweep uses, computed with the factorised
+ * first layer and the fused tensor-core kernel.
+ */
+bm_status bm_mlp_rank_pairs(bm_mlp* m, bm_ctx* ctx, int64_t k, const int32_t* m1, const int32_t* m2, float* out);
+/* out[i] = network(x[i]) for k rows of 128 fp32 inputs (rounded to bf16). */
+bm_status bm_mlp_forward(bm_mlp* m, int64_t k, const float* x, float* out);
+/*
+ * One forward and backward pass over k rows: loss = mean (y - t)^2, grads
+ * (may be NULL) receive dloss/dparams in the parameter layout, then
+ * params -= lr * grads unless lr == 0.
+ */
+bm_status bm_mlp_train_step(bm_mlp* m, int64_t k, const float* x, const float* target, float lr,
+                            float* loss, float* grads);
+/*
+ * Trains on data the engine generates.  First it logs `sweeps` rounds: each
+ * builds the exact profit matrix of ctx's current matching, records per
+ * vertex its best partner plus `extra_partners` candidate-pool partners with
+ * their exact deltas (and the round's features), then advances the matching
+ * with one ordinary bm_sweep.  Then it runs `epochs` passes of SGD (batches
+ * of 1024, learning rate lr) over all logged samples, shuffled afresh each
+ * epoch.  ctx's matching is left where the last logged sweep put it.
+ */
+bm_status bm_mlp_train_from(bm_mlp* m, bm_ctx* ctx, int32_t sweeps, int32_t extra_partners, int32_t epochs,
+                            float lr, uint64_t seed, bm_mlp_train_stats* stats);
+/*
+ * One learned sweep.  The candidate pool holds opts->pool partners per
+ * vertex a, each a vertex b whose image a's G1 neighbours' images point at
+ * (b = pinv(f) for f a G2 neighbour of p(v), v a G1 neighbour of a, on the
+ * matching side of the edge).  The network ranks the pool; exactly evaluated
+ * are either the top opts->top_fraction of the whole pool or each vertex's
+ * opts->per_row best-ranked partners; the improving ones are committed in
+ * (delta desc, lo, hi) order with the exact set commit of bm_sweep.  When none
+ * improves, opts->retries more attempts draw fresh pools, and when those fail
+ * too an exhaustive bm_sweep runs instead (*fell_back = 1).
+ * Stats: deltas_evaluated = exact evaluations, candidates = pool pairs ranked;
+ * phase times ms_prep (features and pool), ms_hub (network ranking),
+ * ms_combine (selection and exact deltas), ms_commit (candidate sort and set
+ * commit); after a fallback ms_total also holds the exhaustive sweep.
+ */
+bm_status bm_learned_sweep(bm_ctx* ctx, bm_mlp* m, const bm_learned_opts* opts, bm_sweep_stats* stats,
+                           int32_t* fell_back);
+
 /* ---- Host utilities: file formats and the synthetic generator ---- */
 
 /* Free memory returned by the readers below. */
