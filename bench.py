@@ -39,6 +39,9 @@ WORKLOADS = {
 }
 OWN_KERNELS_PER_SWEEP = 13  # relabel x5, row_work, hub B build, hub GEMM, profit, combine + reduce, candidates, commit
 CUB_KERNELS_PER_SWEEP = 20  # two 64-bit radix sorts: histogram + exclusive sum + 8 onesweep passes each
+# learned sweep: contribution, dynamic features, column stats, normalise, pool, U/V, fused ranking,
+# score keys, gather, exact deltas, candidate keys, commit (plus two CUB radix sorts)
+OWN_KERNELS_PER_LEARNED_SWEEP = 12
 
 
 def peaks():
@@ -380,26 +383,144 @@ def run_triples(args, world, rank, local, pg):
     E.close()
 
 
+def run_learned(args, world, rank, local, pg):
+    """Time to score, learned vs plain, on the N=18,524 pair (one GPU per
+    replica).  Plain: exhaustive sweeps from the random start until one
+    commits nothing; its final score is the target.  Learned: the network
+    (trained beforehand on exact deltas that the engine logs along a run from
+    another random start; training time reported apart) drives
+    bm_learned_run from the same start until the target is reached.  Each
+    timed step is one descent of each form; values are medians over steps.
+    The untrained network's time to the same target shows what training adds."""
+    import bm
+    import torch
+    torch.cuda.set_device(local)
+    p = dict(WORKLOADS["n18524_e5m"])
+    p["seed"] += rank
+    g = bm.generate(bm.gen_params(**p))
+    n = g["n"]
+    E = bm.Engine.from_pair(g)
+
+    def plain_descent():
+        E.set_mapping(g["map0"])
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sweeps, dev_ms = 0, 0.0
+        while True:
+            st = E.sweep()
+            sweeps += 1
+            dev_ms += st["ms_total"]
+            if st["committed"] == 0 or sweeps >= 2000:
+                break
+        score = E.score()
+        return time.perf_counter() - t0, dev_ms, sweeps, score
+
+    # training: exact deltas logged along a run from another random start
+    rng = np.random.default_rng(1000 + rank)
+    start = np.concatenate([[0], rng.permutation(n) + 1]).astype(np.int32)
+    net = bm.Mlp(seed=13)
+    E.set_mapping(start)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    tstats = net.train_from(E, sweeps=args.train_sweeps, extra_partners=64, epochs=1, lr=1e-2, seed=5)
+    train_s = time.perf_counter() - t0
+    untrained = bm.Mlp(seed=13)
+    opts = dict(pool=64, top_fraction=0.02, probe_every=8)
+
+    def learned_descent(model, target, seed, host_io):
+        m0 = g["map0"]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        E.set_mapping(m0)
+        r = model.learned_run(E, max_sweeps=4000, target_score=target, seed=seed, trace=False, **opts)
+        if host_io:
+            _ = E.get_mapping()
+        return time.perf_counter() - t0, r
+
+    for w in range(args.warmup):
+        plain_descent()
+    target = plain_descent()[3]
+    for w in range(args.warmup):
+        learned_descent(net, target, 100 + w, True)
+    barrier(pg)
+    plain_t, learned_t, untrained_t, runs, plain_info = [], [], [], [], []
+    with Clocks(local) as clk:
+        for k in range(args.steps):
+            pt, pdev, psw, pscore = plain_descent()
+            plain_t.append(pt)
+            plain_info.append((pdev, psw, pscore))
+            lt, r = learned_descent(net, pscore, 200 + k, True)
+            learned_t.append(lt)
+            runs.append(r)
+    barrier(pg)
+    ut, ur = learned_descent(untrained, target, 300, True)
+    # the full learned descent to its own local optimum (no target)
+    E.set_mapping(g["map0"])
+    t0 = time.perf_counter()
+    full = net.learned_run(E, max_sweeps=4000, target_score=0, seed=400, **opts)
+    full_s = time.perf_counter() - t0
+    T_plain = allreduce_max(pg, statistics.median(plain_t))
+    T_learned = allreduce_max(pg, statistics.median(learned_t))
+    if rank == 0:
+        r0 = runs[len(runs) // 2]
+        own_launches = int(statistics.median(r["learned"] * OWN_KERNELS_PER_LEARNED_SWEEP + r["exhaustive"] * OWN_KERNELS_PER_SWEEP
+                                             for r in runs))
+        line = {
+            "metric": "wall seconds to the plain sweep's final score (learned form)", "value": T_learned,
+            "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * T_learned, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "int32 deltas, bf16 network", "data": "synthetic",
+            "config": {"workload": "learned_n18524", "n": n, "e1": int(len(g["src1"])),
+                       "step": "one descent from the random start to the plain form's final score",
+                       "pool": opts["pool"], "top_fraction": opts["top_fraction"],
+                       "probe_every": opts["probe_every"], "l2": "inputs larger than L2",
+                       "parallelism": f"replicas{world}"},
+            "plain": {"seconds": T_plain, "device_ms": plain_info[0][0], "sweeps": plain_info[0][1],
+                      "final_score": plain_info[0][2]},
+            "learned": {"seconds": T_learned, "ratio_to_plain": T_learned / T_plain, "steps": r0["sweeps"],
+                        "learned_sweeps": r0["learned"], "exhaustive_sweeps": r0["exhaustive"],
+                        "device_ms": r0["ms_total"], "score": r0["score_after"], "reached": r0["reached"]},
+            "learned_to_convergence": {"seconds": full_s, "score": full["score_after"], "steps": full["sweeps"],
+                                       "learned_sweeps": full["learned"], "exhaustive_sweeps": full["exhaustive"]},
+            "untrained": {"seconds": ut, "ratio_to_plain": ut / T_plain, "steps": ur["sweeps"],
+                          "reached": ur["reached"]},
+            "training": {"seconds": train_s, "samples": tstats["samples"], "steps": tstats["steps"],
+                         "logged_sweeps": args.train_sweeps, "first_epoch_loss": tstats["first_loss"],
+                         "last_epoch_loss": tstats["last_loss"], "start": "another random matching"},
+            "e2e": {"value": T_learned, "unit": "s", "h2d_bytes_per_step": (n + 1) * 4,
+                    "d2h_bytes_per_step": (n + 1) * 4, "note": "set_mapping and get_mapping inside the timed region"},
+            "gpu_launches": own_launches,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    net.close()
+    untrained.close()
+    E.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--workload", default="n18524_e5m", choices=sorted(WORKLOADS) + ["batch64", "triples"])
+    ap.add_argument("--workload", default="n18524_e5m",
+                    choices=sorted(WORKLOADS) + ["batch64", "triples", "learned"])
+    ap.add_argument("--train-sweeps", type=int, default=40)
     ap.add_argument("--pre-sweeps", type=int, default=50)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     world, rank, local, pg = dist_setup()
     import bm
-    if args.workload in ("batch64", "triples"):
-        (run_batch if args.workload == "batch64" else run_triples)(args, world, rank, local, pg)
+    if args.workload in ("batch64", "triples") or (args.workload == "learned" and args.impl == "engine"):
+        fn = {"batch64": run_batch, "triples": run_triples, "learned": run_learned}[args.workload]
+        fn(args, world, rank, local, pg)
         if pg is not None:
             pg.barrier()
             pg.destroy_process_group()
         return
-    p = dict(WORKLOADS[args.workload])
+    p = dict(WORKLOADS["n18524_e5m" if args.workload == "learned" else args.workload])
     p["seed"] += rank  # independent replica per rank
     g = bm.generate(bm.gen_params(**p))
     if args.impl == "reference":

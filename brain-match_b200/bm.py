@@ -67,6 +67,13 @@ class LearnedOpts(C.Structure):
                 ("retries", C.c_int32), ("reserved", C.c_int32)]
 
 
+class LearnedRunStats(C.Structure):
+    _fields_ = [("sweeps", C.c_int32), ("learned", C.c_int32), ("exhaustive", C.c_int32), ("reached", C.c_int32),
+                ("converged", C.c_int32), ("reserved", C.c_int32), ("score_before", C.c_int64),
+                ("score_after", C.c_int64), ("committed", C.c_int64), ("ms_total", C.c_float),
+                ("ms_learned", C.c_float), ("ms_exhaustive", C.c_float), ("reserved2", C.c_float)]
+
+
 def _p(a):
     return a.ctypes.data_as(C.c_void_p)
 
@@ -128,6 +135,8 @@ def lib():
         L.bm_mlp_train_step.argtypes = [vp, i64, vp, vp, C.c_float, C.POINTER(C.c_float), vp]
         L.bm_mlp_train_from.argtypes = [vp, vp, i32, i32, i32, C.c_float, C.c_uint64, C.POINTER(MlpTrainStats)]
         L.bm_learned_sweep.argtypes = [vp, vp, C.POINTER(LearnedOpts), C.POINTER(SweepStats), C.POINTER(i32)]
+        L.bm_learned_run.argtypes = [vp, vp, C.POINTER(LearnedOpts), i32, i64, i32, C.POINTER(LearnedRunStats),
+                                     vp, vp, vp]
         L.bm_free.argtypes = [vp]
         L.bm_free.restype = None
         L.bm_read_graph_csv.argtypes = [C.c_char_p, C.POINTER(i64), C.POINTER(vp), C.POINTER(vp),
@@ -504,4 +513,25 @@ class Mlp:
         self._chk(lib().bm_learned_sweep(engine.h, self.h, C.byref(o), C.byref(s), C.byref(fb)))
         d = {k: getattr(s, k) for k, _ in SweepStats._fields_ if k != "reserved"}
         d["fell_back"] = fb.value
+        return d
+
+    def learned_run(self, engine, max_sweeps=1000, target_score=0, probe_every=8, pool=64, top_fraction=0.02,
+                    seed=0, per_row=0, retries=0, trace=False):
+        """The learned-proposal descent (bm_learned_run); returns its stats, and
+        with trace=True also per-step arrays score, ms (cumulative) and kind."""
+        o = LearnedOpts(int(pool), int(per_row), float(top_fraction), int(seed), int(retries), 0)
+        st = LearnedRunStats()
+        if trace:
+            sc = np.zeros(max(max_sweeps, 1), np.int64)
+            ms = np.zeros(max(max_sweeps, 1), np.float32)
+            kd = np.zeros(max(max_sweeps, 1), np.int8)
+            ptrs = (_p(sc), _p(ms), _p(kd))
+        else:
+            ptrs = (None, None, None)
+        self._chk(lib().bm_learned_run(engine.h, self.h, C.byref(o), int(max_sweeps), int(target_score),
+                                       int(probe_every), C.byref(st), *ptrs))
+        d = {k: getattr(st, k) for k, _ in LearnedRunStats._fields_ if not k.startswith("reserved")}
+        if trace:
+            k = st.sweeps
+            d.update(trace_score=sc[:k].copy(), trace_ms=ms[:k].copy(), trace_kind=kd[:k].copy())
         return d

@@ -816,7 +816,7 @@ extern "C" bm_status bm_mlp_train_from(bm_mlp* M, bm_ctx* ctx, int32_t sweeps, i
 
 template <bool W16>
 static bm_status learned_impl(bm_ctx* ctx, bm_mlp* M, const bm_learned_opts* o, bm_sweep_stats* stats,
-                              int* fell_back) {
+                              int* fell_back, bool allow_fallback = true) {
     const int n = ctx->n;
     const int P = o && o->pool > 0 ? o->pool : 64;
     const double frac = o && o->top_fraction > 0 ? std::min(o->top_fraction, 1.0) : 0.02;
@@ -919,7 +919,7 @@ static bm_status learned_impl(bm_ctx* ctx, bm_mlp* M, const bm_learned_opts* o, 
         stats->commit_steps = cs.steps;
         stats->commit_carried = cs.carried;
     }
-    if (cs.committed == 0) {  // nothing improving among the proposals: exhaustive sweep
+    if (cs.committed == 0 && allow_fallback) {  // nothing improving among the proposals: exhaustive sweep
         *fell_back = 1;
         bm_sweep_stats fs;
         r = bm_sweep(ctx, nullptr, &fs);
@@ -944,5 +944,67 @@ extern "C" bm_status bm_learned_sweep(bm_ctx* ctx, bm_mlp* M, const bm_learned_o
     cudaStreamSynchronize(M->cs);
     M->cs = M->st;
     if (fell_back) *fell_back = fb;
+    return s;
+}
+
+extern "C" bm_status bm_learned_run(bm_ctx* ctx, bm_mlp* M, const bm_learned_opts* opts, int32_t max_sweeps,
+                                    int64_t target_score, int32_t probe_every, bm_learned_run_stats* out,
+                                    int64_t* trace_score, float* trace_ms, int8_t* trace_kind) {
+    if (!ctx || !M || max_sweeps < 0 || probe_every < 0) return BM_E_INPUT;
+    if (!ctx->mapped) { snprintf(M->err, sizeof M->err, "bm_learned_run: no mapping set"); return BM_E_STATE; }
+    bm_learned_run_stats rs;
+    memset(&rs, 0, sizeof rs);
+    rs.score_before = ctx->score;
+    const int probe = probe_every > 0 ? probe_every : 8;
+    double rate_learned = -1.0, rate_full = -1.0;  // score gained per device-ms, last of each kind
+    int since_learned = 0;
+    bool converged = false;
+    bm_status s = BM_OK;
+    M->cs = ctx->st;
+    for (int step = 0; step < max_sweeps; step++) {
+        if (target_score > 0 && ctx->score >= target_score) { rs.reached = 1; break; }
+        // learned while it gains at least as fast as the exhaustive sweep; the
+        // first step is learned, the second measures the exhaustive rate
+        const bool learned = rate_learned < 0 || (rate_full >= 0 && (rate_learned >= rate_full || since_learned >= probe));
+        bm_sweep_stats st;
+        int kind = 0;
+        if (learned) {
+            int fb = 0;
+            s = ctx->w16 ? learned_impl<true>(ctx, M, opts, &st, &fb, false)
+                         : learned_impl<false>(ctx, M, opts, &st, &fb, false);
+            if (s) break;
+            rate_learned = (double)(st.score_after - st.score_before) / std::max(st.ms_total, 1e-3f);
+            rs.learned++;
+            rs.ms_learned += st.ms_total;
+            since_learned = 0;
+            kind = 1;
+        }
+        if (!learned || st.committed == 0) {  // exhaustive sweep (also the fallback of a fruitless learned one)
+            const long long before = ctx->score;
+            bm_sweep_stats fs;
+            s = bm_sweep(ctx, nullptr, &fs);
+            if (s) { snprintf(M->err, sizeof M->err, "%s", ctx->err); break; }
+            rate_full = (double)(fs.score_after - before) / std::max(fs.ms_total, 1e-3f);
+            rs.exhaustive++;
+            rs.ms_exhaustive += fs.ms_total;
+            if (!learned) since_learned++;
+            if (kind == 1) { st.committed = fs.committed; st.ms_total += fs.ms_total; kind = 2; }
+            else { st = fs; kind = 0; }
+            if (fs.committed == 0) converged = true;
+        }
+        rs.committed += st.committed;
+        rs.ms_total += st.ms_total;
+        if (trace_score) trace_score[rs.sweeps] = ctx->score;
+        if (trace_ms) trace_ms[rs.sweeps] = rs.ms_total;
+        if (trace_kind) trace_kind[rs.sweeps] = (int8_t)kind;
+        rs.sweeps++;
+        if (converged) break;
+    }
+    if (!s && target_score > 0 && ctx->score >= target_score) rs.reached = 1;
+    rs.converged = converged ? 1 : 0;
+    rs.score_after = ctx->score;
+    cudaStreamSynchronize(M->cs);
+    M->cs = M->st;
+    if (out) *out = rs;
     return s;
 }

@@ -422,6 +422,39 @@ bm_status bm_mlp_train_from(bm_mlp* m, bm_ctx* ctx, int32_t sweeps, int32_t extr
 bm_status bm_learned_sweep(bm_ctx* ctx, bm_mlp* m, const bm_learned_opts* opts, bm_sweep_stats* stats,
                            int32_t* fell_back);
 
+/*
+ * The learned-proposal descent: hill-climbs ctx's matching with learned and
+ * exhaustive sweeps until its score reaches target_score (> 0), an exhaustive
+ * sweep commits nothing (a local optimum of the whole swap neighbourhood), or
+ * max_sweeps steps have run.  Schedule: the first step is a learned sweep,
+ * the second an exhaustive one; after that a learned sweep runs while the
+ * last learned sweep gained at least as much score per device-millisecond as
+ * the last exhaustive one, and otherwise exhaustive sweeps run, with one
+ * learned probe after every probe_every (0: 8) exhaustive sweeps in a row.  A
+ * learned sweep that finds nothing is followed by an exhaustive sweep within
+ * the same step.  Every move is judged and committed exactly.
+ * Optional traces (max_sweeps entries each): the score after each step, the
+ * cumulative device milliseconds, the step's kind (0 exhaustive, 1 learned,
+ * 2 learned then exhaustive).
+ */
+typedef struct {
+    int32_t sweeps;       /* steps run                                         */
+    int32_t learned;      /* learned sweeps                                    */
+    int32_t exhaustive;   /* exhaustive sweeps (fallbacks included)            */
+    int32_t reached;      /* 1: the score reached target_score                 */
+    int32_t converged;    /* 1: stopped at a local optimum                     */
+    int32_t reserved;
+    int64_t score_before, score_after;
+    int64_t committed;    /* swaps applied                                     */
+    float ms_total;       /* device time of all steps                          */
+    float ms_learned;     /* of which learned sweeps                           */
+    float ms_exhaustive;  /* of which exhaustive sweeps                        */
+    float reserved2;
+} bm_learned_run_stats;
+bm_status bm_learned_run(bm_ctx* ctx, bm_mlp* m, const bm_learned_opts* opts, int32_t max_sweeps,
+                         int64_t target_score, int32_t probe_every, bm_learned_run_stats* stats,
+                         int64_t* trace_score, float* trace_ms, int8_t* trace_kind);
+
 /* ---- Host utilities: file formats and the synthetic generator ---- */
 
 /* Free memory returned by the readers below. */

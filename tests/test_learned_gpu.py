@@ -232,3 +232,30 @@ def test_trained_network_beats_untrained(cfg0):
                 assert st["fell_back"] == 0
                 gains[trained] = st["score_after"] - st["score_before"]
     assert gains[True] > 1.5 * gains[False], gains
+
+
+def test_learned_run_is_exact_and_stops_where_asked(cfg0):
+    """The learned descent: its final score is the oracle's score of its final
+    matching, its trace rises monotonically, it stops at the target score, and
+    run to the end it stops at an exhaustive sweep that commits nothing."""
+    orc = Oracle.from_pair(cfg0)
+    with bm.Engine.from_pair(cfg0) as eng, bm.Mlp(seed=13) as net:
+        eng.set_mapping(cfg0["map0"])
+        s0 = eng.score()
+        r = net.learned_run(eng, max_sweeps=400, pool=32, seed=3, trace=True)
+        m = eng.get_mapping()
+        assert r["converged"] == 1 and r["score_before"] == s0
+        assert r["score_after"] == eng.score() == orc.score(m)
+        assert r["learned"] >= 1 and r["exhaustive"] >= 1 and r["sweeps"] == len(r["trace_score"])
+        assert np.all(np.diff(np.concatenate([[s0], r["trace_score"]])) >= 0)
+        assert r["trace_kind"][0] in (1, 2) and r["trace_kind"][-1] in (0, 2)
+        assert np.all(np.diff(r["trace_ms"]) > 0)
+        # the last step was an exhaustive sweep that found nothing: a local optimum
+        assert eng.sweep()["committed"] == 0
+        # stopping at a target
+        target = s0 + (r["score_after"] - s0) // 2
+        eng.set_mapping(cfg0["map0"])
+        r2 = net.learned_run(eng, max_sweeps=400, target_score=target, pool=32, seed=3)
+        assert r2["reached"] == 1 and r2["score_after"] >= target
+        assert r2["score_after"] == orc.score(eng.get_mapping())
+        assert r2["sweeps"] <= r["sweeps"]
