@@ -384,8 +384,8 @@ def run_triples(args, world, rank, local, pg):
 
 
 def run_learned(args, world, rank, local, pg):
-    """Time to score, learned vs plain, on the N=18,524 pair (one GPU per
-    replica).  Plain: exhaustive sweeps from the random start until one
+    """Time to score, learned vs plain, on the N=18,524 pair by default
+    (--graph picks another pair; one GPU per replica).  Plain: exhaustive sweeps from the random start until one
     commits nothing; its final score is the target.  Learned: the network
     (trained beforehand on exact deltas that the engine logs along a run from
     another random start; training time reported apart) drives
@@ -395,7 +395,7 @@ def run_learned(args, world, rank, local, pg):
     import bm
     import torch
     torch.cuda.set_device(local)
-    p = dict(WORKLOADS["n18524_e5m"])
+    p = dict(WORKLOADS[args.graph])
     p["seed"] += rank
     g = bm.generate(bm.gen_params(**p))
     n = g["n"]
@@ -470,7 +470,7 @@ def run_learned(args, world, rank, local, pg):
             "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * T_learned, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": "int32 deltas, bf16 network", "data": "synthetic",
-            "config": {"workload": "learned_n18524", "n": n, "e1": int(len(g["src1"])),
+            "config": {"workload": "learned_" + args.graph, "n": n, "e1": int(len(g["src1"])),
                        "step": "one descent from the random start to the plain form's final score",
                        "pool": opts["pool"], "top_fraction": opts["top_fraction"],
                        "probe_every": opts["probe_every"], "l2": "inputs larger than L2",
@@ -507,6 +507,8 @@ def main():
     ap.add_argument("--workload", default="n18524_e5m",
                     choices=sorted(WORKLOADS) + ["batch64", "triples", "learned"])
     ap.add_argument("--train-sweeps", type=int, default=40)
+    ap.add_argument("--graph", default="n18524_e5m", choices=sorted(WORKLOADS),
+                    help="graph pair of the learned workload")
     ap.add_argument("--pre-sweeps", type=int, default=50)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
@@ -520,7 +522,7 @@ def main():
             pg.barrier()
             pg.destroy_process_group()
         return
-    p = dict(WORKLOADS["n18524_e5m" if args.workload == "learned" else args.workload])
+    p = dict(WORKLOADS[args.graph if args.workload == "learned" else args.workload])
     p["seed"] += rank  # independent replica per rank
     g = bm.generate(bm.gen_params(**p))
     if args.impl == "reference":
