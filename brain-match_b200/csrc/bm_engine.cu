@@ -559,10 +559,13 @@ static bm_status stage_commit(bm_ctx* ctx, const bm_sweep_opts* o) {
     const int max_scan = o ? o->max_candidates : 0;
     const int max_verify = o ? o->max_verify : -1;
     const int lim = (max_scan > 0 && max_scan < n) ? max_scan : n;
+    if (!ctx->cinfo) CK(dalloc(ctx, &ctx->cinfo, (size_t)n * 2 * sizeof(int4)));
+    k_cand_info<W16><<<(lim + 255) / 256, 256, 0, ctx->st>>>(view<W16>(ctx), ctx->ckeys_sorted, lim, ctx->cinfo);
+    CK(cudaGetLastError());
     const size_t smem = commit_group_smem(n);
     CK(cudaFuncSetAttribute(k_commit_group<W16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_commit_group<W16><<<1, 1024, smem, ctx->st>>>(view<W16>(ctx), ctx->ckeys_sorted, lim, max_verify,
-                                                    ctx->cstats);
+                                                    ctx->cstats, ctx->cinfo);
     CK(cudaGetLastError());
     return BM_OK;
 }

@@ -39,6 +39,7 @@ struct bm_ctx {
     int* small = nullptr;          // [0]=row counter [1]=ncand [2]=best delta
     unsigned long long* score_acc = nullptr;
     CommitStats* cstats = nullptr;
+    int4* cinfo = nullptr;  // list extents of the sorted candidates (2 per candidate)
     int* scratch_pairs = nullptr;  // pair/triple inputs and outputs (ints)
     long long scratch_cap = 0;
     unsigned* adj = nullptr;       // G1 adjacency bitmap (3-cycles)

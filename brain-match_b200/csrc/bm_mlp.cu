@@ -387,6 +387,7 @@ struct bm_mlp {
     DBuf contrib, F1, F2, fstat, pa, pb, ys, key, key2, idx, idx2, qa, qb, dd, ckeys, tmp, tall, xin;
     DBuf F1s, F2s, ps, eacc;  // training: per-sweep features and matchings, epoch losses
     DBuf U, V;                // factorised first layer, n x 256 each
+    DBuf cinfo;               // list extents of the sorted candidates
     DBuf S1, S2;              // structural features of the context last seen
     unsigned long long static_serial = 0;
     cudaEvent_t e0 = nullptr, e1 = nullptr, ea = nullptr, eb = nullptr, ec = nullptr;
@@ -414,7 +415,7 @@ static void mlp_free(bm_mlp* M) {
     for (void* p : b) if (p) cudaFree(p);
     DBuf* w[] = {&M->contrib, &M->F1, &M->F2, &M->fstat, &M->pa, &M->pb, &M->ys, &M->key, &M->key2, &M->idx,
                  &M->idx2, &M->qa, &M->qb, &M->dd, &M->ckeys, &M->tmp, &M->tall, &M->xin,
-                 &M->F1s, &M->F2s, &M->ps, &M->eacc, &M->U, &M->V, &M->S1, &M->S2};
+                 &M->F1s, &M->F2s, &M->ps, &M->eacc, &M->U, &M->V, &M->S1, &M->S2, &M->cinfo};
     for (DBuf* d : w) d->release();
     for (cudaEvent_t e : {M->e0, M->e1, M->ea, M->eb, M->ec}) if (e) cudaEventDestroy(e);
     if (M->st) cudaStreamDestroy(M->st);
@@ -842,6 +843,7 @@ static bm_status learned_impl(bm_ctx* ctx, bm_mlp* M, const bm_learned_opts* o, 
     MK(M->qb.need((size_t)top * sizeof(int)));
     MK(M->dd.need((size_t)top * sizeof(int)));
     MK(M->ckeys.need((size_t)top * 2 * sizeof(unsigned long long)));
+    MK(M->cinfo.need((size_t)top * 2 * sizeof(int4)));
     int *pa = M->pa.as<int>(), *pb = M->pb.as<int>(), *idx = M->idx.as<int>(), *idx2 = M->idx2.as<int>();
     int *qa = M->qa.as<int>(), *qb = M->qb.as<int>(), *dd = M->dd.as<int>();
     unsigned *key = M->key.as<unsigned>(), *key2 = M->key2.as<unsigned>();
@@ -885,9 +887,10 @@ static bm_status learned_impl(bm_ctx* ctx, bm_mlp* M, const bm_learned_opts* o, 
         MK(cub::DeviceRadixSort::SortKeys(M->tmp.p, tb, ck, ck + top, top, 0, 64, M->cs));
         MK(cudaGetLastError());
         // exact set commit of the improving ones, in (delta desc, lo, hi) order
+        k_cand_info<W16><<<(top + 255) / 256, 256, 0, M->cs>>>(g, ck + top, top, M->cinfo.as<int4>());
         const size_t smem = commit_group_smem(n);
         MK(cudaFuncSetAttribute(k_commit_group<W16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_commit_group<W16><<<1, 1024, smem, M->cs>>>(g, ck + top, top, -1, ctx->cstats);
+        k_commit_group<W16><<<1, 1024, smem, M->cs>>>(g, ck + top, top, -1, ctx->cstats, M->cinfo.as<int4>());
         MK(cudaGetLastError());
         MK(cudaMemcpyAsync(&cs, ctx->cstats, sizeof cs, cudaMemcpyDeviceToHost, M->cs));
         MK(cudaEventRecord(M->e1, M->cs));

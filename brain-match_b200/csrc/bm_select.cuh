@@ -130,7 +130,7 @@ __device__ __forceinline__ void atomicOr_u16(uint16_t* p, uint16_t v) {
 template <bool W16>
 __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsigned long long* __restrict__ keys,
                                              int lim, int max_verify, CommitStats* __restrict__ st,
-                                             unsigned char* smem) {
+                                             unsigned char* smem, const int4* __restrict__ cinfo = nullptr) {
     typedef Ent<W16> EN;
     // shared: used[n] flags, then the matching and the pre-move images as
     // 16-bit ids (n <= 65535, so the "unmatched" value n fits)
@@ -144,13 +144,17 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
     __shared__ unsigned s_imask[kCG];   // earlier pairs of the step G1-adjacent to this one
     __shared__ unsigned s_share[kCG];   // earlier pairs of the step sharing a vertex with this one
     __shared__ unsigned s_dead;         // pairs with a vertex already moved when the step starts
-    __shared__ int s_inf[kCG][7];       // la0, la, ia0, ia, lb0, lb, ib0
+    __shared__ int s_inf[kCG][8];       // la0, la, ia0, ia, lb0, lb, ib0, ib
     __shared__ int s_n, s_k, s_scanned;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     for (int i = tid; i < n; i += blockDim.x) { used[i] = 0; p16[i] = (uint16_t)g.p[i]; mark[i] = 0; }
     if (tid == 0) { s_n = 0; s_k = 0; s_scanned = 0; p16[n] = (uint16_t)n; }
     long long total = 0, entries = 0;
     int verified = 0, committed = 0, steps = 0, carried = 0;
+    int pf_base = -1;                  // warp 0: start of the window prefetched into s_pfkey, s_pfinf
+    __shared__ unsigned long long s_pfkey[32];
+    __shared__ int4 s_pfinf[32][2];
+    __shared__ int s_inf2[kCG][8];     // carried rows in transit
     __syncthreads();
     for (;;) {
         // ---- warp 0: append live candidates after the carried ones, then the
@@ -159,7 +163,15 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
             int cnt = s_n, k = s_k, scanned = s_scanned;
             while (cnt < kCG && k < lim) {
                 const int idx = k + lane;
-                const unsigned long long key = idx < lim ? keys[idx] : ~0ull;
+                unsigned long long key;
+                int4 i0 = make_int4(0, 0, 0, 0), i1 = make_int4(0, 0, 0, 0);
+                if (k == pf_base) {  // the window prefetched at the end of the last step
+                    asm volatile("cp.async.wait_group 0;" ::: "memory");
+                    key = s_pfkey[lane]; i0 = s_pfinf[lane][0]; i1 = s_pfinf[lane][1];
+                } else {
+                    key = idx < lim ? keys[idx] : ~0ull;
+                    if (cinfo && idx < lim) { i0 = cinfo[2 * idx]; i1 = cinfo[2 * idx + 1]; }
+                }
                 const bool valid = key != ~0ull;
                 const int lo = valid ? (int)((key >> 16) & 0xffffu) : 0;
                 const int hi = valid ? (int)(key & 0xffffu) : 0;
@@ -176,25 +188,46 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
                     took = room;
                 }
                 if (live && before < room) {
-                    s_lo[cnt + before] = lo; s_hi[cnt + before] = hi;
-                    s_d0[cnt + before] = (int)(0x7fffffffu - (unsigned)(key >> 32));
+                    const int q = cnt + before;
+                    s_lo[q] = lo; s_hi[q] = hi;
+                    s_d0[q] = (int)(0x7fffffffu - (unsigned)(key >> 32));
+                    if (!cinfo) {  // list extents straight from the offsets
+                        i0.x = g.off1o[lo]; i0.y = g.off1o[lo + 1] - i0.x;
+                        i0.z = g.off1i[lo]; i0.w = g.off1i[lo + 1] - i0.z;
+                        i1.x = g.off1o[hi]; i1.y = g.off1o[hi + 1] - i1.x;
+                        i1.z = g.off1i[hi]; i1.w = g.off1i[hi + 1] - i1.z;
+                    }
+                    s_inf[q][0] = i0.x; s_inf[q][1] = i0.y; s_inf[q][2] = i0.z; s_inf[q][3] = i0.w;
+                    s_inf[q][4] = i1.x; s_inf[q][5] = i1.y; s_inf[q][6] = i1.z; s_inf[q][7] = i1.w;
                 }
                 cnt += took;
                 k += consumed;
                 scanned += consumed;
                 if (consumed == nvalid && nvalid < 32) { k = lim; break; }
             }
+            // prefetch the next window (its keys and list extents); it is used as
+            // is, since only the used flags change and those are read at use
+            if (cinfo) {  // asynchronous copies straight into shared memory, each lane its own slot
+                const int idx = k + lane;
+                pf_base = k;
+                if (idx < lim) {
+                    const uint32_t dk = (uint32_t)__cvta_generic_to_shared(&s_pfkey[lane]);
+                    const uint32_t di = (uint32_t)__cvta_generic_to_shared(&s_pfinf[lane][0]);
+                    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" :: "r"(dk), "l"(keys + idx) : "memory");
+                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(di), "l"(cinfo + 2 * idx) : "memory");
+                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(di + 16), "l"(cinfo + 2 * idx + 1) : "memory");
+                } else {
+                    s_pfkey[lane] = ~0ull;
+                    s_pfinf[lane][0] = make_int4(0, 0, 0, 0);
+                    s_pfinf[lane][1] = make_int4(0, 0, 0, 0);
+                }
+                asm volatile("cp.async.commit_group;" ::: "memory");
+            }
             __syncwarp();
             int len = 0;
             if (lane < cnt) {
                 const int a = s_lo[lane], b = s_hi[lane];
-                const int la0 = g.off1o[a], la = g.off1o[a + 1] - la0;
-                const int ia0 = g.off1i[a], ia = g.off1i[a + 1] - ia0;
-                const int lb0 = g.off1o[b], lb = g.off1o[b + 1] - lb0;
-                const int ib0 = g.off1i[b], ib = g.off1i[b + 1] - ib0;
-                s_inf[lane][0] = la0; s_inf[lane][1] = la; s_inf[lane][2] = ia0; s_inf[lane][3] = ia;
-                s_inf[lane][4] = lb0; s_inf[lane][5] = lb; s_inf[lane][6] = ib0;
-                len = la + ia + lb + ib;
+                len = s_inf[lane][1] + s_inf[lane][3] + s_inf[lane][5] + s_inf[lane][7];
                 s_corr[lane] = 0; s_cnt[lane] = 0; s_imask[lane] = 0;
                 atomicOr_u16(&mark[a], (uint16_t)(1u << lane));
                 atomicOr_u16(&mark[b], (uint16_t)(1u << lane));
@@ -283,50 +316,69 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
         }
         const int my_lo = tid < cnt ? s_lo[tid] : 0, my_hi = tid < cnt ? s_hi[tid] : 0;
         __syncthreads();
-        // ---- clear the step's marks; decide in order (thread 0): register bitmask logic ----
+        // ---- clear the step's marks; decide in order in warp 0: lane j holds pair
+        //      j's fields, every lane replays the same bitmask logic over the
+        //      shuffled fields, then the lanes apply their own outcomes ----
         if (tid < cnt) { mark[my_lo] = 0; mark[my_hi] = 0; }
-        if (tid == 0) {
-            unsigned cm = 0, pm = 0;
-            int np = 0;
-            bool stop = false;
+        if (wid == 0) {
+            const bool in = lane < cnt;
+            const unsigned share = in ? s_share[lane] : 0u, touch = in ? (s_imask[lane] | share) : 0u;
+            const int moved = in ? s_cnt[lane] : 0, corr = in ? s_corr[lane] : 0, d0 = in ? s_d0[lane] : 0;
+            const int a = in ? s_lo[lane] : 0, b = in ? s_hi[lane] : 0;
             const unsigned dead = s_dead;
-            for (int j = 0; j < cnt; j++) {
-                const unsigned share = s_share[j], touch = s_imask[j] | share;
-                const bool is_dead = ((dead >> j) & 1u) || (share & cm);  // a vertex already moved
+            unsigned cm = 0, pm = 0;
+            bool stop = false;
+#pragma unroll
+            for (int j = 0; j < kCG; j++) {
+                const unsigned sh_j = __shfl_sync(0xffffffffu, share, j);
+                const unsigned to_j = __shfl_sync(0xffffffffu, touch, j);
+                const int mv_j = __shfl_sync(0xffffffffu, moved, j);
+                const int co_j = __shfl_sync(0xffffffffu, corr, j);
+                const int d0_j = __shfl_sync(0xffffffffu, d0, j);
+                if (j >= cnt) continue;
+                const bool is_dead = ((dead >> j) & 1u) || (sh_j & cm);  // a vertex already moved
                 bool carry = stop;
                 if (!carry) {
                     if (is_dead) continue;  // decided: skip
-                    if (touch & (cm | pm)) carry = true;
+                    if (to_j & (cm | pm)) carry = true;
                 }
-                const int a = s_lo[j], b = s_hi[j];
                 if (carry) {
                     if (max_verify >= 0) stop = true;
                     carried++;
                     pm |= 1u << j;
-                    s_lo[np] = a; s_hi[np] = b; s_d0[np] = s_d0[j];
-                    np++;
                     continue;
                 }
-                const int moved = s_cnt[j];
-                int d = s_d0[j];
+                int d = d0_j;
                 bool ok = true;
-                if (moved > 0) {
+                if (mv_j > 0) {
                     if (max_verify >= 0 && verified >= max_verify) ok = false;
-                    else { verified++; d += s_corr[j]; }
+                    else { verified++; d += co_j; }
                 }
                 if (ok && d > 0) {
-                    const int fa = p16[a], fb = p16[b];
-                    q16[a] = (uint16_t)fa; q16[b] = (uint16_t)fb;
-                    p16[a] = (uint16_t)fb; p16[b] = (uint16_t)fa;
-                    if (fb < n) g.pinv[fb] = a;
-                    if (fa < n) g.pinv[fa] = b;
-                    used[a] = 1; used[b] = 1;
                     cm |= 1u << j;
                     total += d;
                     committed++;
                 }
             }
-            s_n = np;
+            __syncwarp();
+            if ((cm >> lane) & 1u) {  // committed pairs share no vertex: apply in parallel
+                const int fa = p16[a], fb = p16[b];
+                q16[a] = (uint16_t)fa; q16[b] = (uint16_t)fb;
+                p16[a] = (uint16_t)fb; p16[b] = (uint16_t)fa;
+                if (fb < n) g.pinv[fb] = a;
+                if (fa < n) g.pinv[fa] = b;
+                used[a] = 1; used[b] = 1;
+            }
+            const bool carried_me = (pm >> lane) & 1u;  // carried pairs move to the front, in order
+            const int q = __popc(pm & ((1u << lane) - 1u));
+            if (carried_me)
+                for (int t = 0; t < 8; t++) s_inf2[q][t] = s_inf[lane][t];
+            __syncwarp();
+            if (carried_me) {
+                s_lo[q] = a; s_hi[q] = b; s_d0[q] = d0;
+                for (int t = 0; t < 8; t++) s_inf[q][t] = s_inf2[q][t];
+            }
+            if (lane == 0) s_n = __popc(pm);
         }
         __syncthreads();
     }
@@ -342,6 +394,25 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
     }
 }
 
+// List extents of each sorted candidate for the set commit, two int4 per
+// candidate: (out-offset, out-length, in-offset, in-length) of its lower and of
+// its higher vertex; zeros for the "no candidate" key ~0.
+template <bool W16>
+__global__ void k_cand_info(DevView<W16> g, const unsigned long long* __restrict__ keys, int lim,
+                            int4* __restrict__ info) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= lim) return;
+    const unsigned long long key = keys[i];
+    int4 x = make_int4(0, 0, 0, 0), y = x;
+    if (key != ~0ull) {
+        const int lo = (int)((key >> 16) & 0xffffu), hi = (int)(key & 0xffffu);
+        x.x = g.off1o[lo]; x.y = g.off1o[lo + 1] - x.x; x.z = g.off1i[lo]; x.w = g.off1i[lo + 1] - x.z;
+        y.x = g.off1o[hi]; y.y = g.off1o[hi + 1] - y.x; y.z = g.off1i[hi]; y.w = g.off1i[hi + 1] - y.z;
+    }
+    info[2 * i] = x;
+    info[2 * i + 1] = y;
+}
+
 // Shared memory bytes of commit_group for n vertices.
 __host__ __device__ inline size_t commit_group_smem(int n) {
     return (size_t)((n + 15) & ~15) + 3 * sizeof(uint16_t) * (size_t)((n + 8) & ~7);
@@ -350,9 +421,9 @@ __host__ __device__ inline size_t commit_group_smem(int n) {
 template <bool W16>
 __global__ void __launch_bounds__(1024)
 k_commit_group(DevView<W16> g, const unsigned long long* __restrict__ keys, int lim, int max_verify,
-               CommitStats* __restrict__ st) {
+               CommitStats* __restrict__ st, const int4* __restrict__ cinfo) {
     extern __shared__ unsigned char smem[];
-    commit_group<W16>(g, keys, lim, max_verify, st, smem);
+    commit_group<W16>(g, keys, lim, max_verify, st, smem, cinfo);
 }
 
 }  // namespace bm
