@@ -37,11 +37,12 @@ WORKLOADS = {
     # smaller pair for ncu captures (S = 268 MB, still above L2)
     "n8192_e1m": dict(n=8192, e=1_000_000, wmax=30000, tail_prob=1e-3, seed=20261206),
 }
-OWN_KERNELS_PER_SWEEP = 13  # relabel x5, row_work, hub B build, hub GEMM, profit, combine + reduce, candidates, commit
+OWN_KERNELS_PER_SWEEP = 14  # relabel x5, row_work, hub B build, hub GEMM, profit, combine + reduce, candidates,
+#                             candidate extents, commit
 CUB_KERNELS_PER_SWEEP = 20  # two 64-bit radix sorts: histogram + exclusive sum + 8 onesweep passes each
 # learned sweep: contribution, dynamic features, column stats, normalise, pool, U/V, fused ranking,
-# score keys, gather, exact deltas, candidate keys, commit (plus two CUB radix sorts)
-OWN_KERNELS_PER_LEARNED_SWEEP = 12
+# score keys, gather, exact deltas, candidate keys, candidate extents, commit (plus two CUB radix sorts)
+OWN_KERNELS_PER_LEARNED_SWEEP = 13
 
 
 def peaks():
@@ -247,6 +248,24 @@ def run_engine(args, g, world, rank, local, pg):
         except (OSError, ValueError):
             traffic = None
     terms = statistics.mean(s["min_terms"] for s in stats)
+    # the survey's whole-sweep roofline: T_roof = max(compulsory bytes / HBM peak,
+    # algorithmic min+add / INT32 peak), with the reference's per-delta work
+    # 2 (d(a) + d(b)) summed over all pairs = 4 E (N - 1); the INT32 peak is
+    # measured live by the engine's microbenchmark (independent min+add pairs)
+    try:
+        red_peak, minadd_peak = bm.measure_peaks(n)
+    except Exception:
+        red_peak, minadd_peak = None, None
+    sweep_roof = None
+    if minadd_peak:
+        ops = 4.0 * int(info["e1"]) * (n - 1)
+        t_roof = max(alg_bytes / (peak * 1e9), ops / minadd_peak)
+        t_meas = ms_max / args.steps / 1e3
+        sweep_roof = {"ops_per_sweep": ops, "int32_minadd_peak_per_s": minadd_peak,
+                      "smem_red_peak_per_s": red_peak, "t_roof_ms": 1e3 * t_roof, "t_sweep_ms": 1e3 * t_meas,
+                      "frac": t_roof / t_meas,
+                      "note": "above 1 because the sparse profit matrix skips the zero min terms "
+                              "that the per-pair formula counts"}
 
     if rank == 0:
         cpu = None
@@ -273,6 +292,7 @@ def run_engine(args, g, world, rank, local, pg):
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "kernel": "k_profit", "kernel_ms": prof_ms, "alg_bytes": alg_bytes,
                          "min_terms": terms},
+            "sweep_roofline_int32": sweep_roof,
             "cpu_baseline": cpu,
             "gpu_launches": args.steps * (OWN_KERNELS_PER_SWEEP + CUB_KERNELS_PER_SWEEP),
             "clocks": clk.summary(),

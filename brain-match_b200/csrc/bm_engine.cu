@@ -244,6 +244,7 @@ extern "C" bm_status bm_create(bm_ctx** out, int32_t n, int64_t e1, const int32_
         e = cudaGetDeviceProperties(&prop, ctx->dev);
         if (e != cudaSuccess) { set_err(ctx, "bm_create: %s", cudaGetErrorString(e)); return fail(BM_E_CUDA); }
         ctx->num_sms = prop.multiProcessorCount;
+        ctx->smem_optin = prop.sharedMemPerBlockOptin;
     }
     auto body = [&]() -> bm_status {
         CK(cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking));
@@ -563,6 +564,11 @@ static bm_status stage_commit(bm_ctx* ctx, const bm_sweep_opts* o) {
     k_cand_info<W16><<<(lim + 255) / 256, 256, 0, ctx->st>>>(view<W16>(ctx), ctx->ckeys_sorted, lim, ctx->cinfo);
     CK(cudaGetLastError());
     const size_t smem = commit_group_smem(n);
+    if (smem + 4096 > ctx->smem_optin) {
+        set_err(ctx, "set commit needs %zu bytes of shared memory for n=%d (limit %zu): n too large for a sweep",
+                smem, n, ctx->smem_optin);
+        return BM_E_INPUT;
+    }
     CK(cudaFuncSetAttribute(k_commit_group<W16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_commit_group<W16><<<1, 1024, smem, ctx->st>>>(view<W16>(ctx), ctx->ckeys_sorted, lim, max_verify,
                                                     ctx->cstats, ctx->cinfo);

@@ -13,6 +13,7 @@ struct bm_ctx {
     int n = 0;
     bool w16 = true;
     int dev = 0, num_sms = 0;
+    size_t smem_optin = 0;  // opt-in shared memory per block
     long long e1 = 0, e2 = 0, nself = 0;
     cudaStream_t st = nullptr;
     char err[512] = {0};

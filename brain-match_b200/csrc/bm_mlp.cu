@@ -889,6 +889,11 @@ static bm_status learned_impl(bm_ctx* ctx, bm_mlp* M, const bm_learned_opts* o, 
         // exact set commit of the improving ones, in (delta desc, lo, hi) order
         k_cand_info<W16><<<(top + 255) / 256, 256, 0, M->cs>>>(g, ck + top, top, M->cinfo.as<int4>());
         const size_t smem = commit_group_smem(n);
+        if (smem + 4096 > ctx->smem_optin) {
+            snprintf(M->err, sizeof M->err, "set commit needs %zu bytes of shared memory for n=%d: n too large",
+                     smem, n);
+            return BM_E_INPUT;
+        }
         MK(cudaFuncSetAttribute(k_commit_group<W16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         k_commit_group<W16><<<1, 1024, smem, M->cs>>>(g, ck + top, top, -1, ctx->cstats, M->cinfo.as<int4>());
         MK(cudaGetLastError());

@@ -224,3 +224,22 @@ def test_hub_gemm_heavy_weights_against_oracle():
             O.sweep(m)
             assert np.array_equal(E.get_mapping(), m)
         assert E.score() == O.score(m)
+
+
+def test_sweep_rejects_n_beyond_the_set_commit():
+    """n = 40,000 leaves too little shared memory for the one-CTA set commit
+    (7 bytes per vertex): the sweep says so instead of failing in a launch,
+    while pair deltas and the score still work at that size."""
+    n = 40_000
+    rng = np.random.default_rng(3)
+    s = rng.integers(1, n + 1, 20_000).astype(np.int32)
+    d = rng.integers(1, n + 1, 20_000).astype(np.int32)
+    w = rng.integers(1, 9, 20_000).astype(np.int32)
+    m = np.concatenate([[0], rng.permutation(n) + 1]).astype(np.int32)
+    with bm.Engine(n, s, d, w, d, s, w) as E:
+        E.set_mapping(m)
+        assert E.score() >= 0
+        assert len(E.pair_deltas([1, 2], [3, 4])) == 2
+        with pytest.raises(bm.BMError) as ei:
+            E.sweep()
+        assert ei.value.status == bm.BM_E_INPUT and "too large" in str(ei.value)
