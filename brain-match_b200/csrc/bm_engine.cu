@@ -143,6 +143,7 @@ static void free_ctx(bm_ctx* c) {
     if (c->part) cudaFree(c->part);
     for (void* b : {(void*)c->hubs, (void*)c->is_hub, (void*)c->hubA, (void*)c->hubB, (void*)c->hub_err})
         if (b) cudaFree(b);
+    if (c->cinfo) cudaFree(c->cinfo);
     if (c->ev_hub) cudaEventDestroy(c->ev_hub);
     if (c->st) cudaStreamDestroy(c->st);
     delete c;
