@@ -561,6 +561,14 @@ static bm_status stage_commit(bm_ctx* ctx, const bm_sweep_opts* o) {
     const int max_scan = o ? o->max_candidates : 0;
     const int max_verify = o ? o->max_verify : -1;
     const int lim = (max_scan > 0 && max_scan < n) ? max_scan : n;
+    {   // G1 lists and offsets into L2 for the commit's scattered list reads
+        const size_t es = W16 ? 4 : 8;
+        k_prefetch_l2<<<ctx->num_sms * 4, 256, 0, ctx->st>>>((const char*)ctx->ent1o, (size_t)ctx->e1 * es);
+        k_prefetch_l2<<<ctx->num_sms * 4, 256, 0, ctx->st>>>((const char*)ctx->ent1i, (size_t)ctx->e1 * es);
+        k_prefetch_l2<<<ctx->num_sms, 256, 0, ctx->st>>>((const char*)ctx->off1o, (size_t)(n + 2) * sizeof(int));
+        k_prefetch_l2<<<ctx->num_sms, 256, 0, ctx->st>>>((const char*)ctx->off1i, (size_t)(n + 2) * sizeof(int));
+        CK(cudaGetLastError());
+    }
     if (!ctx->cinfo) CK(dalloc(ctx, &ctx->cinfo, (size_t)n * 2 * sizeof(int4)));
     k_cand_info<W16><<<(lim + 255) / 256, 256, 0, ctx->st>>>(view<W16>(ctx), ctx->ckeys_sorted, lim, ctx->cinfo);
     CK(cudaGetLastError());

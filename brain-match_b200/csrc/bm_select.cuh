@@ -145,6 +145,8 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
     __shared__ unsigned s_share[kCG];   // earlier pairs of the step sharing a vertex with this one
     __shared__ unsigned s_dead;         // pairs with a vertex already moved when the step starts
     __shared__ int s_inf[kCG][8];       // la0, la, ia0, ia, lb0, lb, ib0, ib
+    __shared__ int s_segpre[4 * kCG + 1];  // the step's lists as segments 4j + k: prefix of their lengths
+    __shared__ int s_segoff[4 * kCG];      // first entry of segment 4j + k in ent1o (k even) or ent1i (k odd)
     __shared__ int s_n, s_k, s_scanned;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     for (int i = tid; i < n; i += blockDim.x) { used[i] = 0; p16[i] = (uint16_t)g.p[i]; mark[i] = 0; }
@@ -242,6 +244,19 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
                 if (lane >= o) incl += y;
             }
             if (lane < cnt) s_pre[lane + 1] = incl;
+            __syncwarp();
+            {   // segment table: lane = segment 4j + k (a out, a in, b out, b in of pair j)
+                const int j = lane >> 2, k = lane & 3;
+                const int slen = j < cnt ? s_inf[j][2 * k + 1] : 0;
+                int sincl = slen;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, sincl, o);
+                    if (lane >= o) sincl += y;
+                }
+                s_segpre[lane + 1] = sincl;
+                s_segoff[lane] = j < cnt ? s_inf[j][2 * k] : 0;
+                if (lane == 0) s_segpre[0] = 0;
+            }
             const unsigned dead = __ballot_sync(0xffffffffu, lane < cnt && (used[s_lo[lane < cnt ? lane : 0]] | used[s_hi[lane < cnt ? lane : 0]]));
             if (lane == 0) {
                 s_pre[0] = 0; s_dead = dead;
@@ -261,26 +276,30 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
             constexpr int kMLP = 4;
             const int tot = s_pre[cnt];
             // every thread runs the same number of rounds, so warp collectives are safe
+            const int nseg = 4 * cnt;
             for (int base = 0; base < tot; base += kMLP * blockDim.x) {
                 int jj[kMLP], kind[kMLP];
                 typename EN::T en[kMLP];
+                // this thread's kMLP consecutive entries: one segment search, then
+                // step to the next segment where a list ends (coalesced per warp)
+                const int e0 = base + kMLP * tid;
+                int seg = 0;
+                if (e0 < tot) {
+                    int lo = 0, hi = nseg;  // s_segpre[lo] <= e0 < s_segpre[hi]
+                    while (hi - lo > 1) { const int mid = (lo + hi) >> 1; if (s_segpre[mid] <= e0) lo = mid; else hi = mid; }
+                    seg = lo;
+                }
 #pragma unroll
                 for (int u = 0; u < kMLP; u++) {
-                    const int e = base + tid + u * blockDim.x;
+                    const int e = e0 + u;
                     jj[u] = -1;
                     kind[u] = 0;
                     if (e >= tot) continue;
-                    int lo = 0, hi = cnt;  // s_pre[lo] <= e < s_pre[hi]
-                    while (hi - lo > 1) { const int mid = (lo + hi) >> 1; if (s_pre[mid] <= e) lo = mid; else hi = mid; }
-                    const int j = lo;
-                    int q = e - s_pre[j];
-                    const typename EN::T* src;
-                    if (q < s_inf[j][1]) { src = g.ent1o + s_inf[j][0] + q; kind[u] = 0; }
-                    else if ((q -= s_inf[j][1]) < s_inf[j][3]) { src = g.ent1i + s_inf[j][2] + q; kind[u] = 1; }
-                    else if ((q -= s_inf[j][3]) < s_inf[j][5]) { src = g.ent1o + s_inf[j][4] + q; kind[u] = 2; }
-                    else { q -= s_inf[j][5]; src = g.ent1i + s_inf[j][6] + q; kind[u] = 3; }
+                    while (e >= s_segpre[seg + 1]) seg++;
+                    const typename EN::T* src = ((seg & 1) ? g.ent1i : g.ent1o) + s_segoff[seg] + (e - s_segpre[seg]);
                     en[u] = *src;
-                    jj[u] = j;
+                    jj[u] = seg >> 2;
+                    kind[u] = seg & 3;
                 }
                 int wv[kMLP][4];
                 bool mv[kMLP];
@@ -392,6 +411,16 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
         st->entries = entries;
         st->carried = carried;
     }
+}
+
+// Pulls [p, p + bytes) into L2 (one prefetch per 128-byte line).  The set
+// commit reads G1 list entries of scattered vertices from a single CTA; the
+// profit matrix traffic before it has evicted those lists, so without this
+// every first touch of a list goes to HBM.
+static __global__ void k_prefetch_l2(const char* __restrict__ p, size_t bytes) {
+    const size_t lines = (bytes + 127) / 128;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < lines; i += (size_t)gridDim.x * blockDim.x)
+        asm volatile("prefetch.global.L2 [%0];" :: "l"(p + i * 128));
 }
 
 // List extents of each sorted candidate for the set commit, two int4 per
