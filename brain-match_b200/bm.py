@@ -33,7 +33,8 @@ class Info(C.Structure):
 
 
 class SweepOpts(C.Structure):
-    _fields_ = [("max_candidates", C.c_int32), ("max_verify", C.c_int32), ("reserved", C.c_int32 * 6)]
+    _fields_ = [("max_candidates", C.c_int32), ("max_verify", C.c_int32), ("commit_ctas", C.c_int32),
+                ("reserved", C.c_int32 * 5)]
 
 
 class SweepStats(C.Structure):
@@ -268,8 +269,8 @@ class Engine:
         _check(lib().bm_profit_row(self.h, int(a), _p(out)), self.h)
         return out
 
-    def sweep(self, max_candidates=0, max_verify=-1):
-        o = SweepOpts(max_candidates, max_verify)
+    def sweep(self, max_candidates=0, max_verify=-1, commit_ctas=0):
+        o = SweepOpts(max_candidates, max_verify, commit_ctas)
         s = SweepStats()
         _check(lib().bm_sweep(self.h, C.byref(o), C.byref(s)), self.h)
         return {k: getattr(s, k) for k, _ in SweepStats._fields_ if k != "reserved"}

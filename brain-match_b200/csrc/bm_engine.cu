@@ -144,6 +144,7 @@ static void free_ctx(bm_ctx* c) {
     for (void* b : {(void*)c->hubs, (void*)c->is_hub, (void*)c->hubA, (void*)c->hubB, (void*)c->hub_err})
         if (b) cudaFree(b);
     if (c->cinfo) cudaFree(c->cinfo);
+    if (c->cgrid) cudaFree(c->cgrid);
     if (c->ev_hub) cudaEventDestroy(c->ev_hub);
     if (c->st) cudaStreamDestroy(c->st);
     delete c;
@@ -578,10 +579,14 @@ static bm_status stage_commit(bm_ctx* ctx, const bm_sweep_opts* o) {
                 smem, n, ctx->smem_optin);
         return BM_E_INPUT;
     }
-    CK(cudaFuncSetAttribute(k_commit_group<W16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_commit_group<W16><<<1, 1024, smem, ctx->st>>>(view<W16>(ctx), ctx->ckeys_sorted, lim, max_verify,
-                                                    ctx->cstats, ctx->cinfo);
-    CK(cudaGetLastError());
+    int ctas = o && o->commit_ctas > 0 ? o->commit_ctas : kCommitDefaultCtas;
+    ctas = std::min(std::min(ctas, kCommitMaxCtas), ctx->num_sms);
+    if (!ctx->cgrid) {
+        CK(dalloc(ctx, &ctx->cgrid, commit_grid_ints() * sizeof(int)));
+        CK(cudaMemset(ctx->cgrid, 0, commit_grid_ints() * sizeof(int)));
+    }
+    CK(launch_commit_group<W16>(view<W16>(ctx), ctx->ckeys_sorted, lim, max_verify, ctx->cstats, ctx->cinfo, ctas,
+                                ctx->cgrid, smem, ctx->st));
     return BM_OK;
 }
 
@@ -636,13 +641,16 @@ extern "C" bm_status bm_sweep(bm_ctx* ctx, const bm_sweep_opts* opts, bm_sweep_s
     CommitStats cs;
     int small[3];
     unsigned long long terms = 0;
-    int herr = 0;
+    int herr = 0, cerr = 0;
     CK(cudaMemcpyAsync(&cs, ctx->cstats, sizeof cs, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaMemcpyAsync(small, ctx->small, 3 * sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaMemcpyAsync(&terms, ctx->work_sum, sizeof terms, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaMemcpyAsync(&herr, ctx->hub_err, sizeof herr, cudaMemcpyDeviceToHost, ctx->st));
+    if (ctx->cgrid)
+        CK(cudaMemcpyAsync(&cerr, ctx->cgrid, sizeof cerr, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     if (herr) { set_err(ctx, "bm_sweep: tensor-core hub GEMM wait timed out"); return BM_E_TIMEOUT; }
+    if (cerr) { set_err(ctx, "bm_sweep: set commit grid barrier wait timed out"); return BM_E_TIMEOUT; }
     ctx->score = before + cs.total_delta;
     if (stats) {
         memset(stats, 0, sizeof *stats);

@@ -41,6 +41,7 @@ struct bm_ctx {
     unsigned long long* score_acc = nullptr;
     CommitStats* cstats = nullptr;
     int4* cinfo = nullptr;  // list extents of the sorted candidates (2 per candidate)
+    int* cgrid = nullptr;   // set commit across CTAs: partial sums [2][32][8][3], barrier [2], error [1]
     int* scratch_pairs = nullptr;  // pair/triple inputs and outputs (ints)
     long long scratch_cap = 0;
     unsigned* adj = nullptr;       // G1 adjacency bitmap (3-cycles)

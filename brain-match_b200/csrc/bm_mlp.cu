@@ -894,12 +894,19 @@ static bm_status learned_impl(bm_ctx* ctx, bm_mlp* M, const bm_learned_opts* o, 
                      smem, n);
             return BM_E_INPUT;
         }
-        MK(cudaFuncSetAttribute(k_commit_group<W16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_commit_group<W16><<<1, 1024, smem, M->cs>>>(g, ck + top, top, -1, ctx->cstats, M->cinfo.as<int4>());
-        MK(cudaGetLastError());
+        if (!ctx->cgrid) {
+            MK(cudaMalloc(&ctx->cgrid, commit_grid_ints() * sizeof(int)));
+            MK(cudaMemset(ctx->cgrid, 0, commit_grid_ints() * sizeof(int)));
+        }
+        const int ctas = std::min(kCommitDefaultCtas, ctx->num_sms);
+        MK(launch_commit_group<W16>(g, ck + top, top, -1, ctx->cstats, M->cinfo.as<int4>(), ctas, ctx->cgrid, smem,
+                                    M->cs));
         MK(cudaMemcpyAsync(&cs, ctx->cstats, sizeof cs, cudaMemcpyDeviceToHost, M->cs));
+        int cerr = 0;
+        MK(cudaMemcpyAsync(&cerr, ctx->cgrid, sizeof cerr, cudaMemcpyDeviceToHost, M->cs));
         MK(cudaEventRecord(M->e1, M->cs));
         if ((r = check_err(M))) return r;
+        if (cerr) { snprintf(M->err, sizeof M->err, "set commit grid barrier wait timed out"); return BM_E_TIMEOUT; }
         if (stats) {
             float t[5];
             cudaEventElapsedTime(&t[0], M->e0, M->ea);

@@ -125,12 +125,58 @@ __device__ __forceinline__ void atomicOr_u16(uint16_t* p, uint16_t v) {
     atomicOr(w, (unsigned)v << ((addr & 2) ? 16 : 0));
 }
 
+// Several CTAs on one set commit, as one thread-block cluster: every CTA keeps
+// the same shared state and makes the same gather and the same ordered
+// decisions; only the step's list scan is divided.  Each CTA publishes its
+// per-pair partial sums in its own shared memory (two buffers, by step
+// parity), arrives on every CTA's step mbarrier, waits on its own (bounded),
+// and reads the others' partials through distributed shared memory.
+struct CommitGrid {
+    int nct;          // CTAs of the cluster (1: a single CTA, no exchange)
+    int* err;         // bit 1 set when a cluster wait runs out
+};
+
+__device__ __forceinline__ uint32_t cluster_map(uint32_t local_addr, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(local_addr), "r"(rank));
+    return r;
+}
+
+// Arrive on the step mbarrier of every CTA of the cluster, then wait (bounded)
+// for this CTA's to complete the phase; false on timeout.  Thread 0 of each
+// CTA does the arrivals and the wait; the CTA syncs around it.
+__device__ __forceinline__ bool cluster_step_sync(uint32_t bar, uint32_t phase, int nct, int* err) {
+    __shared__ int s_cok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int r = 0; r < nct; r++) {
+            const uint32_t rb = cluster_map(bar, (uint32_t)r);
+            asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" :: "r"(rb) : "memory");
+        }
+        int ok = 0;
+        for (int it = 0; it < (1 << 22); it++) {
+            uint32_t done;
+            asm volatile(
+                "{\n\t.reg .pred p;\n\t"
+                "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+                "selp.u32 %0, 1, 0, p;\n\t}"
+                : "=r"(done) : "r"(bar), "r"(phase) : "memory");
+            if (done) { ok = 1; break; }
+        }
+        if (!ok) atomicOr(err, 2);
+        s_cok = ok;
+    }
+    __syncthreads();
+    return s_cok != 0;
+}
+
 // The set commit of one instance; all 1024 threads of the block call it.
 // smem: commit_group_smem(n) bytes of dynamic shared memory.
 template <bool W16>
 __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsigned long long* __restrict__ keys,
                                              int lim, int max_verify, CommitStats* __restrict__ st,
-                                             unsigned char* smem, const int4* __restrict__ cinfo = nullptr) {
+                                             unsigned char* smem, const int4* __restrict__ cinfo = nullptr,
+                                             CommitGrid grid = CommitGrid{1, nullptr}) {
     typedef Ent<W16> EN;
     // shared: used[n] flags, then the matching and the pre-move images as
     // 16-bit ids (n <= 65535, so the "unmatched" value n fits)
@@ -149,6 +195,23 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
     __shared__ int s_segoff[4 * kCG];      // first entry of segment 4j + k in ent1o (k even) or ent1i (k odd)
     __shared__ int s_n, s_k, s_scanned;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int nct = grid.nct;
+    int ct = 0;
+    if (nct > 1) asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(ct));
+    int gstep = 0;      // steps taken, the same in every CTA
+    bool aborted = false;
+    __shared__ __align__(8) unsigned long long s_cbar;   // the step mbarrier (nct arrivals per phase)
+    __shared__ int s_cpart[2][kCG][3];                   // this CTA's partial sums, by step parity
+    const uint32_t cbar = (uint32_t)__cvta_generic_to_shared(&s_cbar);
+    if (nct > 1) {
+        if (tid == 0) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(cbar), "r"(nct) : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        // every CTA's mbarrier is initialised before anyone arrives on it
+        asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+        asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
+    }
     for (int i = tid; i < n; i += blockDim.x) { used[i] = 0; p16[i] = (uint16_t)g.p[i]; mark[i] = 0; }
     if (tid == 0) { s_n = 0; s_k = 0; s_scanned = 0; p16[n] = (uint16_t)n; }
     long long total = 0, entries = 0;
@@ -274,10 +337,11 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
         //      thread resolves kMLP entries and issues their loads together ----
         {
             constexpr int kMLP = 4;
-            const int tot = s_pre[cnt];
-            // every thread runs the same number of rounds, so warp collectives are safe
+            const int all = s_pre[cnt];
+            // this CTA's slice of the step's entries
+            const int first = (int)((long long)all * ct / nct), tot = (int)((long long)all * (ct + 1) / nct);
             const int nseg = 4 * cnt;
-            for (int base = 0; base < tot; base += kMLP * blockDim.x) {
+            for (int base = first; base < tot; base += kMLP * blockDim.x) {
                 int jj[kMLP], kind[kMLP];
                 typename EN::T en[kMLP];
                 // this thread's kMLP consecutive entries: one segment search, then
@@ -335,6 +399,30 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
         }
         const int my_lo = tid < cnt ? s_lo[tid] : 0, my_hi = tid < cnt ? s_hi[tid] : 0;
         __syncthreads();
+        if (nct > 1) {  // exchange the per-pair partial sums of the CTAs' slices
+            const int buf = gstep & 1;
+            if (tid < cnt) {
+                s_cpart[buf][tid][0] = s_corr[tid]; s_cpart[buf][tid][1] = s_cnt[tid];
+                s_cpart[buf][tid][2] = (int)s_imask[tid];
+            }
+            if (!cluster_step_sync(cbar, (uint32_t)buf, nct, grid.err)) { aborted = true; break; }
+            if (tid < cnt) {
+                int corr = 0, moved = 0;
+                unsigned im = 0;
+                const uint32_t mine = (uint32_t)__cvta_generic_to_shared(&s_cpart[buf][tid][0]);
+                for (int c = 0; c < nct; c++) {  // the same order in every CTA
+                    const uint32_t q = cluster_map(mine, (uint32_t)c);
+                    int v0, v1, v2;
+                    asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v0) : "r"(q) : "memory");
+                    asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v1) : "r"(q + 4) : "memory");
+                    asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v2) : "r"(q + 8) : "memory");
+                    corr += v0; moved |= v1; im |= (unsigned)v2;
+                }
+                s_corr[tid] = corr; s_cnt[tid] = moved; s_imask[tid] = im;
+            }
+            __syncthreads();
+        }
+        gstep++;
         // ---- clear the step's marks; decide in order in warp 0: lane j holds pair
         //      j's fields, every lane replays the same bitmask logic over the
         //      shuffled fields, then the lanes apply their own outcomes ----
@@ -384,8 +472,10 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
                 const int fa = p16[a], fb = p16[b];
                 q16[a] = (uint16_t)fa; q16[b] = (uint16_t)fb;
                 p16[a] = (uint16_t)fb; p16[b] = (uint16_t)fa;
-                if (fb < n) g.pinv[fb] = a;
-                if (fa < n) g.pinv[fa] = b;
+                if (ct == 0) {
+                    if (fb < n) g.pinv[fb] = a;
+                    if (fa < n) g.pinv[fa] = b;
+                }
                 used[a] = 1; used[b] = 1;
             }
             const bool carried_me = (pm >> lane) & 1u;  // carried pairs move to the front, in order
@@ -401,6 +491,8 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
         }
         __syncthreads();
     }
+    if (nct > 1 && !aborted) cluster_step_sync(cbar, (uint32_t)(gstep & 1), nct, grid.err);
+    if (ct != 0) return;
     for (int i = tid; i < n; i += blockDim.x) g.p[i] = p16[i];
     if (tid == 0) {
         st->total_delta = total;
@@ -442,6 +534,19 @@ __global__ void k_cand_info(DevView<W16> g, const unsigned long long* __restrict
     info[2 * i + 1] = y;
 }
 
+constexpr int kCommitMaxCtas = 8;      // a portable cluster
+constexpr int kCommitDefaultCtas = 4;
+// The set commit's error word (one int; bit 1: a cluster wait ran out).
+__host__ __device__ inline size_t commit_grid_ints() { return 4; }
+
+// Launches the set commit on `ctas` CTAs forming one thread-block cluster (a
+// plain launch for one); `buf` holds commit_grid_ints() ints: the error word,
+// reset here.  Returns the launch status.
+template <bool W16>
+__host__ inline cudaError_t launch_commit_group(const DevView<W16>& g, const unsigned long long* keys, int lim,
+                                               int max_verify, CommitStats* st, const int4* cinfo, int ctas,
+                                               int* buf, size_t smem, cudaStream_t stream);
+
 // Shared memory bytes of commit_group for n vertices.
 __host__ __device__ inline size_t commit_group_smem(int n) {
     return (size_t)((n + 15) & ~15) + 3 * sizeof(uint16_t) * (size_t)((n + 8) & ~7);
@@ -450,9 +555,37 @@ __host__ __device__ inline size_t commit_group_smem(int n) {
 template <bool W16>
 __global__ void __launch_bounds__(1024)
 k_commit_group(DevView<W16> g, const unsigned long long* __restrict__ keys, int lim, int max_verify,
-               CommitStats* __restrict__ st, const int4* __restrict__ cinfo) {
+               CommitStats* __restrict__ st, const int4* __restrict__ cinfo, CommitGrid grid) {
     extern __shared__ unsigned char smem[];
-    commit_group<W16>(g, keys, lim, max_verify, st, smem, cinfo);
+    commit_group<W16>(g, keys, lim, max_verify, st, smem, cinfo, grid);
+}
+
+template <bool W16>
+__host__ inline cudaError_t launch_commit_group(const DevView<W16>& g, const unsigned long long* keys, int lim,
+                                               int max_verify, CommitStats* st, const int4* cinfo, int ctas,
+                                               int* buf, size_t smem, cudaStream_t stream) {
+    cudaError_t e = cudaFuncSetAttribute(k_commit_group<W16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    CommitGrid grid{1, buf};
+    if (ctas <= 1) {
+        k_commit_group<W16><<<1, 1024, smem, stream>>>(g, keys, lim, max_verify, st, cinfo, grid);
+        return cudaGetLastError();
+    }
+    grid.nct = ctas;
+    if ((e = cudaMemsetAsync(grid.err, 0, sizeof(int), stream)) != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(ctas);
+    cfg.blockDim = dim3(1024);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = ctas;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_commit_group<W16>, g, keys, lim, max_verify, st, cinfo, grid);
 }
 
 }  // namespace bm

@@ -166,7 +166,10 @@ bm_status bm_profit_row(bm_ctx* ctx, int32_t a, int32_t* out);
 typedef struct {
     int32_t max_candidates;  /* sorted candidates scanned per sweep (<=0: all)   */
     int32_t max_verify;      /* re-verifications of tainted candidates (<0: all) */
-    int32_t reserved[6];
+    int32_t commit_ctas;     /* CTAs (one thread-block cluster) sharing the set
+                                commit's list scans: 0 = default (4), 1..8;
+                                results never depend on it                      */
+    int32_t reserved[5];
 } bm_sweep_opts;
 
 typedef struct {

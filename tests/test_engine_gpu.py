@@ -243,3 +243,25 @@ def test_sweep_rejects_n_beyond_the_set_commit():
         with pytest.raises(bm.BMError) as ei:
             E.sweep()
         assert ei.value.status == bm.BM_E_INPUT and "too large" in str(ei.value)
+
+
+@pytest.mark.parametrize("flags", [0, bm.BM_FLAG_FORCE_I32])
+def test_commit_across_ctas_is_identical(cfg0, flags):
+    """The set commit split over 1, 2, 8 or 32 CTAs (list scans divided, the
+    same ordered decisions in every CTA) commits exactly the same swaps, with
+    and without a re-verification budget, and matches the oracle."""
+    orc = oracle.Oracle.from_pair(cfg0)
+    for max_verify in (-1, 40):
+        maps = []
+        for ctas in (1, 2, 8, 32):
+            with bm.Engine.from_pair(cfg0, flags) as E:
+                E.set_mapping(cfg0["map0"])
+                for _ in range(4):
+                    E.sweep(max_verify=max_verify, commit_ctas=ctas)
+                maps.append(E.get_mapping())
+        for m in maps[1:]:
+            np.testing.assert_array_equal(m, maps[0])
+        m = cfg0["map0"].copy()
+        for _ in range(4):
+            orc.sweep(m, max_verify=max_verify)
+        np.testing.assert_array_equal(maps[0], m)
