@@ -139,6 +139,13 @@ __device__ __forceinline__ void scatter_list(int* acc, const typename Ent<W16>::
     typedef Ent<W16> EN;
     typedef typename EN::T E;
     int i = i0 + first;
+    for (; i + 7 * step < i1; i += 8 * step) {  // eight loads in flight per thread
+        E x[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) x[u] = list[i + u * step];
+#pragma unroll
+        for (int u = 0; u < 8; u++) atomicAdd(&acc[EN::id(x[u])], imin(w1, EN::w(x[u])));
+    }
     for (; i + 3 * step < i1; i += 4 * step) {
         const E x0 = list[i], x1 = list[i + step], x2 = list[i + 2 * step], x3 = list[i + 3 * step];
         atomicAdd(&acc[EN::id(x0)], imin(w1, EN::w(x0)));
@@ -195,28 +202,51 @@ __device__ __forceinline__ void profit_row(const DevView<W16>& g, int a, int* ac
     // out-edges of a against G2 in-lists of p(v), then in-edges against out-lists of p(u)
     const int so = g.off1o[a], lo = g.off1o[a + 1] - so;
     const int si = g.off1i[a], li = g.off1i[a + 1] - si;
-    for (int j = wid; j < lo + li; j += nw) {
-        const bool out = j < lo;
-        const E ea = out ? g.ent1oP[so + j] : g.ent1iP[si + (j - lo)];
-        const int f = EN::id(ea), w1 = EN::w(ea);
-        const int* off = out ? g.off2i : g.off2o;
-        const E* list = out ? g.ent2iP : g.ent2oP;
-        const int b0 = off[f], b1 = off[f + 1];
-        if (!out && is_hub && is_hub[EN::id(g.ent1i[si + (j - lo)])]) {
-            if (w1 > hub_thr)
-                scatter_residual<W16>(acc, g.ent2oHP, g.off2oH[f], g.off2oH[f + 1], w1, hub_thr, lane, 32);
-            continue;
-        }
-        if (b1 - b0 > kLongList) {
-            int q = 0;
-            if (lane == 0) q = atomicAdd(s_nlong, 1);
-            q = __shfl_sync(0xffffffffu, q, 0);
-            if (q < kLongQueue) {
-                if (lane == 0) s_long[q] = make_int2(f, w1 | (out ? 0 : (int)0x80000000));
-                continue;
+    // the warp's edges are j = wid + nw * t; lane t loads the set-up of its t-th
+    // edge (entry, list extent, kind) so one round of loads serves 32 edges
+    const int tot = lo + li;
+    for (int base = wid; base < tot; base += nw * 32) {
+        const int j = base + nw * lane;
+        int f = 0, w1 = 0, b0 = 0, b1 = 0, kind = 0;  // kind: 0 none, 1 out-edge, 2 in-edge, 3 hub residual
+        if (j < tot) {
+            const bool out = j < lo;
+            const E ea = out ? g.ent1oP[so + j] : g.ent1iP[si + (j - lo)];
+            f = EN::id(ea);
+            w1 = EN::w(ea);
+            if (!out && is_hub && is_hub[EN::id(g.ent1i[si + (j - lo)])]) {
+                // hub in-edge: the GEMM has its terms up to the threshold
+                if (w1 > hub_thr) { kind = 3; b0 = g.off2oH[f]; b1 = g.off2oH[f + 1]; }
+            } else {
+                kind = out ? 1 : 2;
+                const int* off = out ? g.off2i : g.off2o;
+                b0 = off[f];
+                b1 = off[f + 1];
             }
         }
-        scatter_list<W16>(acc, list, b0, b1, w1, lane, 32);
+        const int cnt = min(32, (tot - base + nw - 1) / nw);
+        for (int t = 0; t < cnt; t++) {
+            const int kt = __shfl_sync(0xffffffffu, kind, t);
+            const int w1t = __shfl_sync(0xffffffffu, w1, t);
+            const int b0t = __shfl_sync(0xffffffffu, b0, t);
+            const int b1t = __shfl_sync(0xffffffffu, b1, t);
+            const int ft = __shfl_sync(0xffffffffu, f, t);
+            if (kt == 0) continue;
+            if (kt == 3) {
+                scatter_residual<W16>(acc, g.ent2oHP, b0t, b1t, w1t, hub_thr, lane, 32);
+                continue;
+            }
+            const bool out = kt == 1;
+            if (b1t - b0t > kLongList) {
+                int q = 0;
+                if (lane == 0) q = atomicAdd(s_nlong, 1);
+                q = __shfl_sync(0xffffffffu, q, 0);
+                if (q < kLongQueue) {
+                    if (lane == 0) s_long[q] = make_int2(ft, w1t | (out ? 0 : (int)0x80000000));
+                    continue;
+                }
+            }
+            scatter_list<W16>(acc, out ? g.ent2iP : g.ent2oP, b0t, b1t, w1t, lane, 32);
+        }
     }
     __syncthreads();
     // long lists, one at a time, by the whole block

@@ -148,11 +148,11 @@ __device__ __forceinline__ uint32_t cluster_map(uint32_t local_addr, uint32_t ra
 __device__ __forceinline__ bool cluster_step_sync(uint32_t bar, uint32_t phase, int nct, int* err) {
     __shared__ int s_cok;
     __syncthreads();
+    if (threadIdx.x < (unsigned)nct) {  // thread r arrives on CTA r's mbarrier
+        const uint32_t rb = cluster_map(bar, threadIdx.x);
+        asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" :: "r"(rb) : "memory");
+    }
     if (threadIdx.x == 0) {
-        for (int r = 0; r < nct; r++) {
-            const uint32_t rb = cluster_map(bar, (uint32_t)r);
-            asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" :: "r"(rb) : "memory");
-        }
         int ok = 0;
         for (int it = 0; it < (1 << 22); it++) {
             uint32_t done;
@@ -405,20 +405,18 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
                 s_cpart[buf][tid][0] = s_corr[tid]; s_cpart[buf][tid][1] = s_cnt[tid];
                 s_cpart[buf][tid][2] = (int)s_imask[tid];
             }
+            if (tid < cnt) { s_corr[tid] = 0; s_cnt[tid] = 0; s_imask[tid] = 0; }
             if (!cluster_step_sync(cbar, (uint32_t)buf, nct, grid.err)) { aborted = true; break; }
-            if (tid < cnt) {
-                int corr = 0, moved = 0;
-                unsigned im = 0;
-                const uint32_t mine = (uint32_t)__cvta_generic_to_shared(&s_cpart[buf][tid][0]);
-                for (int c = 0; c < nct; c++) {  // the same order in every CTA
-                    const uint32_t q = cluster_map(mine, (uint32_t)c);
-                    int v0, v1, v2;
-                    asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v0) : "r"(q) : "memory");
-                    asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v1) : "r"(q + 4) : "memory");
-                    asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v2) : "r"(q + 8) : "memory");
-                    corr += v0; moved |= v1; im |= (unsigned)v2;
-                }
-                s_corr[tid] = corr; s_cnt[tid] = moved; s_imask[tid] = im;
+            if (tid < nct * cnt) {  // thread (c, j): CTA c's partials of pair j (integer sums: any order)
+                const int c = tid / cnt, j = tid - c * cnt;
+                const uint32_t q = cluster_map((uint32_t)__cvta_generic_to_shared(&s_cpart[buf][j][0]), (uint32_t)c);
+                int v0, v1, v2;
+                asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v0) : "r"(q) : "memory");
+                asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v1) : "r"(q + 4) : "memory");
+                asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v2) : "r"(q + 8) : "memory");
+                if (v0) atomicAdd(&s_corr[j], v0);
+                if (v1) atomicOr(&s_cnt[j], v1);
+                if (v2) atomicOr(&s_imask[j], (unsigned)v2);
             }
             __syncthreads();
         }
@@ -535,7 +533,7 @@ __global__ void k_cand_info(DevView<W16> g, const unsigned long long* __restrict
 }
 
 constexpr int kCommitMaxCtas = 8;      // a portable cluster
-constexpr int kCommitDefaultCtas = 4;
+constexpr int kCommitDefaultCtas = 8;
 // The set commit's error word (one int; bit 1: a cluster wait ran out).
 __host__ __device__ inline size_t commit_grid_ints() { return 4; }
 

@@ -167,7 +167,7 @@ typedef struct {
     int32_t max_candidates;  /* sorted candidates scanned per sweep (<=0: all)   */
     int32_t max_verify;      /* re-verifications of tainted candidates (<0: all) */
     int32_t commit_ctas;     /* CTAs (one thread-block cluster) sharing the set
-                                commit's list scans: 0 = default (4), 1..8;
+                                commit's list scans: 0 = default (8), 1..8;
                                 results never depend on it                      */
     int32_t reserved[5];
 } bm_sweep_opts;
