@@ -10,6 +10,7 @@
 //   skip a pair whose vertex already moved, re-evaluate it on the current
 //   matching, commit iff > 0), several pairs per step.
 #pragma once
+#include <climits>
 #include "bm_kernels.cuh"
 
 namespace bm {
@@ -41,27 +42,33 @@ __device__ __forceinline__ void combine_tile(const int* __restrict__ S, int n, i
     }
     __syncthreads();
     const bool diag = (ti == tj);
-    unsigned long long cb[CL];
+    // bests as 32-bit (delta, partner) pairs -- larger delta, then smaller
+    // partner -- packed into the 64-bit key only for the reductions
+    int cbd[CL], cbi[CL];
 #pragma unroll
-    for (int q = 0; q < CL; q++) cb[q] = 0;
+    for (int q = 0; q < CL; q++) { cbd[q] = INT_MIN; cbi[q] = INT_MAX; }
     for (int r = wid; r < T; r += 8) {
         const int a = a0 + r;
-        unsigned long long rb = 0;
+        int rd = INT_MIN, ri = INT_MAX;
         if (a < n) {
 #pragma unroll
             for (int q = 0; q < CL; q++) {
                 const int c = lane + 32 * q, b = b0 + c;
                 if (b < n && b != a) {
                     const int d = sA[r][c] + sB[c][r] - dA[r] - dB[c];
-                    rb = kmax(rb, pack_best(d, b));
-                    cb[q] = kmax(cb[q], pack_best(d, a));
+                    if (d > rd || (d == rd && b < ri)) { rd = d; ri = b; }
+                    if (d > cbd[q] || (d == cbd[q] && a < cbi[q])) { cbd[q] = d; cbi[q] = a; }
                     if (all_out && a < b) all_out[(long long)a * (2LL * n - a - 1) / 2 + (b - a - 1)] = d;
                 }
             }
         }
+        unsigned long long rb = ri == INT_MAX ? 0ull : pack_best(rd, ri);
         for (int o = 16; o; o >>= 1) rb = kmax(rb, __shfl_xor_sync(0xffffffffu, rb, o));
         if (lane == 0 && a < n) part[(size_t)tj * n + a] = rb;  // row partial of a over this tile
     }
+    unsigned long long cb[CL];
+#pragma unroll
+    for (int q = 0; q < CL; q++) cb[q] = cbi[q] == INT_MAX ? 0ull : pack_best(cbd[q], cbi[q]);
     // column partials (vertices b of the tile, over this tile's rows); a
     // diagonal tile's row partials already cover both orders of every pair
     if (!diag) {
