@@ -186,7 +186,7 @@ k_b_commit(const DevView<W16>* __restrict__ views, const BatchInst* __restrict__
     const DevView<W16> g = views[b];
     const BatchInst I = inst[b];
     const int lim = (max_scan > 0 && max_scan < I.n) ? max_scan : I.n;
-    commit_group<W16>(g, I.keys_sorted, lim, max_verify, &st[b], smem);
+    commit_group<W16, kCGBatch>(g, I.keys_sorted, lim, max_verify, &st[b], smem);
     __syncthreads();
     if (threadIdx.x == 0) {
         acc_delta[b] += st[b].total_delta;

@@ -111,7 +111,7 @@ static __global__ void k_best_reduce(const unsigned long long* __restrict__ part
 //     a pair with at least one moved neighbour is the "re-verified" case
 //     (counted, and limited by max_verify);
 //   * commit iff the current delta is > 0.
-// It is executed kCG pairs at a time: the CTA makes one coalesced pass over
+// It is executed CG pairs at a time: the CTA makes one coalesced pass over
 // the step's edge lists (entries spread evenly over all threads, so a hub
 // pair does not stall the step), accumulating each pair's correction
 // from moved neighbours (a flag check per entry; W2 is read only for moved
@@ -123,7 +123,8 @@ static __global__ void k_best_reduce(const unsigned long long* __restrict__ part
 // every decision equals the one-at-a-time rule's.  With a re-verification
 // budget the step stops at the first carried pair, so the budget is spent in
 // the sequential order.
-constexpr int kCG = 8;                 // pairs per step
+constexpr int kCG = 16;                // pairs per step of the cluster commit (at most 16: marks are 16-bit)
+constexpr int kCGBatch = 8;            // pairs per step of a one-CTA commit (batched instances)
 
 // 16-bit atomic OR in shared memory through the aligned 32-bit word.
 __device__ __forceinline__ void atomicOr_u16(uint16_t* p, uint16_t v) {
@@ -179,7 +180,7 @@ __device__ __forceinline__ bool cluster_step_sync(uint32_t bar, uint32_t phase, 
 
 // The set commit of one instance; all 1024 threads of the block call it.
 // smem: commit_group_smem(n) bytes of dynamic shared memory.
-template <bool W16>
+template <bool W16, int CG = kCG>
 __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsigned long long* __restrict__ keys,
                                              int lim, int max_verify, CommitStats* __restrict__ st,
                                              unsigned char* smem, const int4* __restrict__ cinfo = nullptr,
@@ -192,14 +193,14 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
     uint16_t* p16 = reinterpret_cast<uint16_t*>(smem + ((n + 15) & ~15));
     uint16_t* q16 = p16 + ((n + 8) & ~7);
     uint16_t* mark = q16 + ((n + 8) & ~7);  // bit i set: vertex belongs to pair i of the step
-    __shared__ int s_lo[kCG], s_hi[kCG], s_d0[kCG];
-    __shared__ int s_corr[kCG], s_cnt[kCG], s_pre[kCG + 1];
-    __shared__ unsigned s_imask[kCG];   // earlier pairs of the step G1-adjacent to this one
-    __shared__ unsigned s_share[kCG];   // earlier pairs of the step sharing a vertex with this one
+    __shared__ int s_lo[CG], s_hi[CG], s_d0[CG];
+    __shared__ int s_corr[CG], s_cnt[CG], s_pre[CG + 1];
+    __shared__ unsigned s_imask[CG];   // earlier pairs of the step G1-adjacent to this one
+    __shared__ unsigned s_share[CG];   // earlier pairs of the step sharing a vertex with this one
     __shared__ unsigned s_dead;         // pairs with a vertex already moved when the step starts
-    __shared__ int s_inf[kCG][8];       // la0, la, ia0, ia, lb0, lb, ib0, ib
-    __shared__ int s_segpre[4 * kCG + 1];  // the step's lists as segments 4j + k: prefix of their lengths
-    __shared__ int s_segoff[4 * kCG];      // first entry of segment 4j + k in ent1o (k even) or ent1i (k odd)
+    __shared__ int s_inf[CG][8];       // la0, la, ia0, ia, lb0, lb, ib0, ib
+    __shared__ int s_segpre[4 * CG + 1];  // the step's lists as segments 4j + k: prefix of their lengths
+    __shared__ int s_segoff[4 * CG];      // first entry of segment 4j + k in ent1o (k even) or ent1i (k odd)
     __shared__ int s_n, s_k, s_scanned;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const int nct = grid.nct;
@@ -208,7 +209,7 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
     int gstep = 0;      // steps taken, the same in every CTA
     bool aborted = false;
     __shared__ __align__(8) unsigned long long s_cbar;   // the step mbarrier (nct arrivals per phase)
-    __shared__ int s_cpart[2][kCG][3];                   // this CTA's partial sums, by step parity
+    __shared__ int s_cpart[2][CG][3];                   // this CTA's partial sums, by step parity
     const uint32_t cbar = (uint32_t)__cvta_generic_to_shared(&s_cbar);
     if (nct > 1) {
         if (tid == 0) {
@@ -226,14 +227,14 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
     int pf_base = -1;                  // warp 0: start of the window prefetched into s_pfkey, s_pfinf
     __shared__ unsigned long long s_pfkey[32];
     __shared__ int4 s_pfinf[32][2];
-    __shared__ int s_inf2[kCG][8];     // carried rows in transit
+    __shared__ int s_inf2[CG][8];     // carried rows in transit
     __syncthreads();
     for (;;) {
         // ---- warp 0: append live candidates after the carried ones, then the
         //      per-pair list extents and their prefix (lane j = pair j) ----
         if (wid == 0) {
             int cnt = s_n, k = s_k, scanned = s_scanned;
-            while (cnt < kCG && k < lim) {
+            while (cnt < CG && k < lim) {
                 const int idx = k + lane;
                 unsigned long long key;
                 int4 i0 = make_int4(0, 0, 0, 0), i1 = make_int4(0, 0, 0, 0);
@@ -250,7 +251,7 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
                 const bool live = valid && !used[lo] && !used[hi];
                 const unsigned vmask = __ballot_sync(0xffffffffu, valid);
                 const unsigned lmask = __ballot_sync(0xffffffffu, live);
-                const int room = kCG - cnt;
+                const int room = CG - cnt;
                 const int before = __popc(lmask & ((1u << lane) - 1u));
                 const int nvalid = __popc(vmask);  // valid keys form a prefix
                 int consumed = nvalid, took = __popc(lmask);
@@ -315,16 +316,22 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
             }
             if (lane < cnt) s_pre[lane + 1] = incl;
             __syncwarp();
-            {   // segment table: lane = segment 4j + k (a out, a in, b out, b in of pair j)
-                const int j = lane >> 2, k = lane & 3;
-                const int slen = j < cnt ? s_inf[j][2 * k + 1] : 0;
-                int sincl = slen;
-                for (int o = 1; o < 32; o <<= 1) {
-                    const int y = __shfl_up_sync(0xffffffffu, sincl, o);
-                    if (lane >= o) sincl += y;
+            {   // segment table: segment 4j + k (a out, a in, b out, b in of pair j), 32 per pass
+                int carry = 0;
+                for (int h = 0; h < (4 * CG + 31) / 32; h++) {
+                    const int seg = lane + 32 * h, j = seg >> 2, k = seg & 3;
+                    const int slen = j < cnt ? s_inf[j][2 * k + 1] : 0;
+                    int sincl = slen;
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int y = __shfl_up_sync(0xffffffffu, sincl, o);
+                        if (lane >= o) sincl += y;
+                    }
+                    if (seg < 4 * CG) {
+                        s_segpre[seg + 1] = carry + sincl;
+                        s_segoff[seg] = j < cnt ? s_inf[j][2 * k] : 0;
+                    }
+                    carry += __shfl_sync(0xffffffffu, sincl, 31);
                 }
-                s_segpre[lane + 1] = sincl;
-                s_segoff[lane] = j < cnt ? s_inf[j][2 * k] : 0;
                 if (lane == 0) s_segpre[0] = 0;
             }
             const unsigned dead = __ballot_sync(0xffffffffu, lane < cnt && (used[s_lo[lane < cnt ? lane : 0]] | used[s_hi[lane < cnt ? lane : 0]]));
@@ -441,7 +448,7 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
             unsigned cm = 0, pm = 0;
             bool stop = false;
 #pragma unroll
-            for (int j = 0; j < kCG; j++) {
+            for (int j = 0; j < CG; j++) {
                 const unsigned sh_j = __shfl_sync(0xffffffffu, share, j);
                 const unsigned to_j = __shfl_sync(0xffffffffu, touch, j);
                 const int mv_j = __shfl_sync(0xffffffffu, moved, j);
