@@ -37,9 +37,9 @@ WORKLOADS = {
     # smaller pair for ncu captures (S = 268 MB, still above L2)
     "n8192_e1m": dict(n=8192, e=1_000_000, wmax=30000, tail_prob=1e-3, seed=20261206),
 }
-OWN_KERNELS_PER_SWEEP = 14  # relabel x5, row_work, hub B build, hub GEMM, profit, combine + reduce, candidates,
-#                             candidate extents, commit
-CUB_KERNELS_PER_SWEEP = 20  # two 64-bit radix sorts: histogram + exclusive sum + 8 onesweep passes each
+OWN_KERNELS_PER_SWEEP = 18  # relabel x5, row_work, hub B build, hub GEMM, profit, combine + reduce, candidates,
+#                             4 L2 prefetches, candidate extents, commit
+CUB_KERNELS_PER_SWEEP = 16  # two radix sorts: histogram + exclusive sum + 6 onesweep passes each
 # learned sweep: contribution, dynamic features, column stats, normalise, pool, U/V, fused ranking,
 # score keys, gather, exact deltas, candidate keys, candidate extents, commit (plus two CUB radix sorts)
 OWN_KERNELS_PER_LEARNED_SWEEP = 13
@@ -66,7 +66,7 @@ class Clocks:
                 ["nvidia-smi", "-i", str(self.dev),
                  "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
                  "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-                 "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "200"],
+                 "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
@@ -204,6 +204,7 @@ def run_engine(args, g, world, rank, local, pg):
     deltas_per_sweep = n * (n - 1) // 2
     for _ in range(args.warmup):
         E.sweep()
+    m_start = E.get_mapping()  # the e2e leg replays the timed sweeps from here
     barrier(pg)
     torch.cuda.synchronize()
     stats = []
@@ -219,9 +220,10 @@ def run_engine(args, g, world, rank, local, pg):
     value = world * args.steps * deltas_per_sweep / (ms_max / 1e3)
 
     # end to end through the C ABI with host buffers: H2D of the matching,
-    # sweep, D2H of the matching and the score
-    host_map = E.get_mapping()
-    e2e_steps = max(3, args.steps)
+    # sweep, D2H of the matching and the score -- the same sweeps as the timed
+    # region, replayed from the same starting matching
+    host_map = m_start
+    e2e_steps = args.steps
     barrier(pg)
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
@@ -521,7 +523,7 @@ def run_learned(args, world, rank, local, pg):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--workload", default="n18524_e5m",
