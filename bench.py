@@ -405,6 +405,53 @@ def run_triples(args, world, rank, local, pg):
     E.close()
 
 
+def run_quads(args, world, rank, local, pg):
+    """4-set permutation rounds on the N=18,524 pair, from the pairwise
+    sweep's output matching (up to 50 sweeps, untimed): 64 connected 4-sets
+    (3-step walks) per vertex, all 23 permutations of each evaluated exactly,
+    best disjoint set committed."""
+    import bm
+    import torch
+    torch.cuda.set_device(local)
+    p = dict(WORKLOADS["n18524_e5m"])
+    p["seed"] += rank
+    g = bm.generate(bm.gen_params(**p))
+    E = bm.Engine.from_pair(g)
+    E.set_mapping(g["map0"])
+    for _ in range(args.pre_sweeps):
+        if E.sweep()["committed"] == 0:
+            break
+    start_score = E.score()
+    for r in range(args.warmup):
+        E.quad_round(partners=64, seed=1000 + r)
+    barrier(pg)
+    torch.cuda.synchronize()
+    stats = []
+    with Clocks(local) as clk:
+        E.timer_mark(0)
+        for r in range(args.steps):
+            stats.append(E.quad_round(partners=64, seed=2000 + r))
+        E.timer_mark(1)
+        torch.cuda.synchronize()
+    barrier(pg)
+    ms = allreduce_max(pg, E.timer_elapsed(0, 1))
+    perms = sum(s["permutations"] for s in stats)
+    if rank == 0:
+        line = {
+            "metric": "exact 4-set permutation deltas/s", "value": world * perms / (ms / 1e3),
+            "unit": "permutations/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "int32", "data": "synthetic",
+            "config": {"workload": "quads_n18524", "partners": 64, "pre_sweeps": args.pre_sweeps,
+                       "start_score": start_score, "step": "one 4-set round (23 permutations per set)"},
+            "rounds": [{k: s[k] for k in ("quads", "committed", "verified", "score_after", "ms_sample",
+                                         "ms_eval", "ms_commit", "ms_total")} for s in stats],
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    E.close()
+
+
 def run_learned(args, world, rank, local, pg):
     """Time to score, learned vs plain, on the N=18,524 pair by default
     (--graph picks another pair; one GPU per replica).  Plain: exhaustive sweeps from the random start until one
@@ -527,7 +574,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--workload", default="n18524_e5m",
-                    choices=sorted(WORKLOADS) + ["batch64", "triples", "learned"])
+                    choices=sorted(WORKLOADS) + ["batch64", "triples", "quads", "learned"])
     ap.add_argument("--train-sweeps", type=int, default=40)
     ap.add_argument("--graph", default="n18524_e5m", choices=sorted(WORKLOADS),
                     help="graph pair of the learned workload")
@@ -537,8 +584,8 @@ def main():
     args = ap.parse_args()
     world, rank, local, pg = dist_setup()
     import bm
-    if args.workload in ("batch64", "triples") or (args.workload == "learned" and args.impl == "engine"):
-        fn = {"batch64": run_batch, "triples": run_triples, "learned": run_learned}[args.workload]
+    if args.workload in ("batch64", "triples", "quads") or (args.workload == "learned" and args.impl == "engine"):
+        fn = {"batch64": run_batch, "triples": run_triples, "quads": run_quads, "learned": run_learned}[args.workload]
         fn(args, world, rank, local, pg)
         if pg is not None:
             pg.barrier()

@@ -75,6 +75,19 @@ class LearnedRunStats(C.Structure):
                 ("ms_learned", C.c_float), ("ms_exhaustive", C.c_float), ("reserved2", C.c_float)]
 
 
+class QuadOpts(C.Structure):
+    _fields_ = [("partners", C.c_int32), ("max_candidates", C.c_int32), ("max_verify", C.c_int32),
+                ("reserved0", C.c_int32), ("seed", C.c_uint64), ("reserved", C.c_int32 * 4)]
+
+
+class QuadStats(C.Structure):
+    _fields_ = [("score_before", C.c_int64), ("score_after", C.c_int64), ("quads", C.c_int64),
+                ("permutations", C.c_int64), ("candidates", C.c_int32), ("scanned", C.c_int32),
+                ("verified", C.c_int32), ("committed", C.c_int32), ("best_delta", C.c_int32),
+                ("reserved", C.c_int32), ("ms_sample", C.c_float), ("ms_eval", C.c_float),
+                ("ms_commit", C.c_float), ("ms_total", C.c_float)]
+
+
 def _p(a):
     return a.ctypes.data_as(C.c_void_p)
 
@@ -138,6 +151,8 @@ def lib():
         L.bm_learned_sweep.argtypes = [vp, vp, C.POINTER(LearnedOpts), C.POINTER(SweepStats), C.POINTER(i32)]
         L.bm_learned_run.argtypes = [vp, vp, C.POINTER(LearnedOpts), i32, i64, i32, C.POINTER(LearnedRunStats),
                                      vp, vp, vp]
+        L.bm_quad_deltas.argtypes = [vp, i64, vp, vp, vp]
+        L.bm_quad_round.argtypes = [vp, C.POINTER(QuadOpts), C.POINTER(QuadStats)]
         L.bm_free.argtypes = [vp]
         L.bm_free.restype = None
         L.bm_read_graph_csv.argtypes = [C.c_char_p, C.POINTER(i64), C.POINTER(vp), C.POINTER(vp),
@@ -293,6 +308,20 @@ class Engine:
         out = np.zeros(2 * len(a), np.int32)
         _check(lib().bm_triple_deltas(self.h, len(a), _p(a), _p(b), _p(c), _p(out)), self.h)
         return out.reshape(-1, 2)
+
+    def quad_deltas(self, sets, perms):
+        """Exact deltas of permutation perms[i] (1..23) of 1-based 4-sets sets[i]."""
+        sets = np.ascontiguousarray(sets, np.int32).reshape(-1, 4)
+        perms = np.ascontiguousarray(perms, np.int32)
+        out = np.zeros(len(sets), np.int32)
+        _check(lib().bm_quad_deltas(self.h, len(sets), _p(sets), _p(perms), _p(out)), self.h)
+        return out
+
+    def quad_round(self, partners=64, seed=0, max_candidates=0, max_verify=-1):
+        o = QuadOpts(partners, max_candidates, max_verify, 0, seed)
+        s = QuadStats()
+        _check(lib().bm_quad_round(self.h, C.byref(o), C.byref(s)), self.h)
+        return {k: getattr(s, k) for k, _ in QuadStats._fields_ if k != "reserved"}
 
     def triple_round(self, partners=256, seed=0, max_candidates=0, max_verify=-1):
         o = TripleOpts()

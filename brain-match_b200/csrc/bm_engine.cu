@@ -17,6 +17,7 @@
 #include "bm.h"
 #include "bm_internal.cuh"
 #include "bm_triples.cuh"
+#include "bm_quads.cuh"
 #include "bm_select.cuh"
 #include "bm_hub.cuh"
 
@@ -856,6 +857,106 @@ extern "C" bm_status bm_triple_round(bm_ctx* ctx, const bm_triple_opts* opts, bm
     if (!ctx || !opts) return BM_E_INPUT;
     if (!ctx->mapped) { set_err(ctx, "bm_triple_round: no mapping set"); return BM_E_STATE; }
     return ctx->w16 ? triple_round_impl<true>(ctx, opts, stats) : triple_round_impl<false>(ctx, opts, stats);
+}
+
+extern "C" bm_status bm_quad_deltas(bm_ctx* ctx, int64_t k, const int32_t* sets, const int32_t* perms,
+                                    int32_t* out) {
+    if (!ctx) return BM_E_INPUT;
+    if (!ctx->mapped) { set_err(ctx, "bm_quad_deltas: no mapping set"); return BM_E_STATE; }
+    if (k < 0 || (k && (!sets || !perms || !out))) { set_err(ctx, "bm_quad_deltas: bad arguments"); return BM_E_INPUT; }
+    if (k == 0) return BM_OK;
+    const int n = ctx->n;
+    std::vector<int> h(5 * k);
+    for (int64_t i = 0; i < k; i++) {
+        const int* v = sets + 4 * i;
+        bool ok = perms[i] >= 1 && perms[i] <= 23;
+        for (int t = 0; t < 4 && ok; t++) {
+            if (v[t] < 1 || v[t] > n) ok = false;
+            for (int u = 0; u < t; u++) if (v[u] == v[t]) ok = false;
+        }
+        if (!ok) {
+            set_err(ctx, "bm_quad_deltas: set %lld = (%d,%d,%d,%d) with permutation %d invalid", (long long)i,
+                    v[0], v[1], v[2], v[3], perms[i]);
+            return BM_E_INPUT;
+        }
+        for (int t = 0; t < 4; t++) h[4 * i + t] = v[t] - 1;
+        h[4 * k + i] = perms[i];
+    }
+    bm_status s = ensure_scratch(ctx, 6 * k);
+    if (s) return s;
+    int* d = ctx->scratch_pairs;
+    CK(cudaMemcpyAsync(d, h.data(), 5 * k * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+    const long long blocks = std::min<long long>((k + 7) / 8, (long long)ctx->num_sms * 16);
+    if (ctx->w16) k_quad_deltas<true><<<(int)blocks, 256, 0, ctx->st>>>(view<true>(ctx), d, d + 4 * k, k, d + 5 * k);
+    else k_quad_deltas<false><<<(int)blocks, 256, 0, ctx->st>>>(view<false>(ctx), d, d + 4 * k, k, d + 5 * k);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, d + 5 * k, k * sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return BM_OK;
+}
+
+template <bool W16>
+static bm_status quad_round_impl(bm_ctx* ctx, const bm_quad_opts* o, bm_quad_stats* stats) {
+    const int n = ctx->n;
+    const int partners = o->partners > 0 ? o->partners : 64;
+    if (partners > 2048) { set_err(ctx, "bm_quad_round: partners=%d above 2048", partners); return BM_E_INPUT; }
+    bm_status s = ensure_S(ctx);
+    if (s) return s;
+    s = ensure_adj<W16>(ctx);
+    if (s) return s;
+    if (!ctx->tcount) CK(dalloc(ctx, &ctx->tcount, 2 * sizeof(unsigned long long)));
+    const long long before = ctx->score;
+    CK(cudaEventRecord(ctx->ev[0], ctx->st));
+    s = stage_profit<W16>(ctx);
+    if (s) return s;
+    CK(cudaEventRecord(ctx->ev[1], ctx->st));
+    CK(cudaMemsetAsync(ctx->tcount, 0, 2 * sizeof(unsigned long long), ctx->st));
+    const int blocks = std::min(n, ctx->num_sms * 8);
+    k_quad_eval<W16><<<blocks, 256, 0, ctx->st>>>(view<W16>(ctx), ctx->adj, ctx->adj_words, partners, o->seed,
+                                                  ctx->ckeys, ctx->tcount);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ctx->ev[2], ctx->st));
+    size_t tb = ctx->cub_bytes;
+    CK(cub::DeviceRadixSort::SortKeys(ctx->cub_tmp, tb, ctx->ckeys, ctx->ckeys_sorted, n, 0, 64, ctx->st));
+    const size_t smem = 2 * (size_t)n;
+    CK(cudaFuncSetAttribute(k_quad_commit<W16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_quad_commit<W16><<<1, 1024, smem, ctx->st>>>(view<W16>(ctx), ctx->ckeys_sorted, n, o->max_candidates,
+                                                    o->max_verify, o->seed, ctx->cstats);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ctx->ev[3], ctx->st));
+    CommitStats cs;
+    unsigned long long cnt[2];
+    std::vector<unsigned long long> keys(n);
+    CK(cudaMemcpyAsync(&cs, ctx->cstats, sizeof cs, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(cnt, ctx->tcount, sizeof cnt, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(keys.data(), ctx->ckeys_sorted, n * sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    ctx->score = before + cs.total_delta;
+    if (stats) {
+        memset(stats, 0, sizeof *stats);
+        stats->score_before = before;
+        stats->score_after = ctx->score;
+        stats->quads = (long long)cnt[0];
+        stats->permutations = 23 * (long long)cnt[0];
+        int nc = 0;
+        while (nc < n && keys[nc] != ~0ull) nc++;
+        stats->candidates = nc;
+        stats->best_delta = nc ? (int)(0x7fffffffu - (unsigned)(keys[0] >> 32)) : 0;
+        stats->scanned = cs.scanned;
+        stats->verified = cs.verified;
+        stats->committed = cs.committed;
+        cudaEventElapsedTime(&stats->ms_sample, ctx->ev[0], ctx->ev[1]);
+        cudaEventElapsedTime(&stats->ms_eval, ctx->ev[1], ctx->ev[2]);
+        cudaEventElapsedTime(&stats->ms_commit, ctx->ev[2], ctx->ev[3]);
+        cudaEventElapsedTime(&stats->ms_total, ctx->ev[0], ctx->ev[3]);
+    }
+    return BM_OK;
+}
+
+extern "C" bm_status bm_quad_round(bm_ctx* ctx, const bm_quad_opts* opts, bm_quad_stats* stats) {
+    if (!ctx || !opts) return BM_E_INPUT;
+    if (!ctx->mapped) { set_err(ctx, "bm_quad_round: no mapping set"); return BM_E_STATE; }
+    return ctx->w16 ? quad_round_impl<true>(ctx, opts, stats) : quad_round_impl<false>(ctx, opts, stats);
 }
 
 // ---------------------------------------------------------------------------

@@ -278,6 +278,48 @@ typedef struct {
  */
 bm_status bm_triple_round(bm_ctx* ctx, const bm_triple_opts* opts, bm_triple_stats* stats);
 
+/* ---- 4-set permutations ---- */
+
+/*
+ * Exact deltas of permuting the images of 4-vertex sets: set i is
+ * sets[4i..4i+3] (distinct 1-based ids), perms[i] in 1..23 is the q-th
+ * permutation of (0,1,2,3) in lexicographic order (0 would be the identity),
+ * and vertex sets[4i+t] takes the image of vertex sets[4i+perm_q[t]].  The
+ * k = 4 case of generate_permutations (src/permutation.c:700-744), scored
+ * like calculate_permutation_delta (:623-696).
+ */
+bm_status bm_quad_deltas(bm_ctx* ctx, int64_t k, const int32_t* sets, const int32_t* perms, int32_t* out);
+
+typedef struct {
+    int32_t partners;        /* 3-step walk samples per vertex (64, at most 2048) */
+    int32_t max_candidates;  /* sorted candidates scanned (<=0: all)              */
+    int32_t max_verify;      /* re-verifications (<0: all)                        */
+    int32_t reserved0;
+    uint64_t seed;           /* round seed for the sampler                        */
+    int32_t reserved[4];
+} bm_quad_opts;
+
+typedef struct {
+    int64_t score_before, score_after;
+    int64_t quads;              /* valid sampled 4-sets                 */
+    int64_t permutations;       /* 23 per 4-set                         */
+    int32_t candidates, scanned, verified, committed;
+    int32_t best_delta, reserved;
+    float   ms_sample, ms_eval, ms_commit, ms_total;
+} bm_quad_stats;
+
+/*
+ * One 4-set round: sample `partners` connected 4-sets per vertex a (a 3-step
+ * walk a -> b -> c -> d along undirected G1 edges), evaluate all 23
+ * non-identity permutations of their images exactly (from the profit matrix
+ * plus the set's internal edges), keep each vertex's best, and commit the best
+ * vertex-disjoint improving sets under the re-verification rule of
+ * bm_triple_round.  The reference enumerates all k-subsets for this
+ * (src/permutation.c:746-800); sampling connected sets keeps it exact per
+ * move and linear in n per round.
+ */
+bm_status bm_quad_round(bm_ctx* ctx, const bm_quad_opts* opts, bm_quad_stats* stats);
+
 /* ---- Batches of independent instances ---- */
 
 /*

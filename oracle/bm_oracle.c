@@ -12,7 +12,9 @@
  *                          after a pass without a commit
  *   orc_triple_local   calculate_permutation_delta src/permutation.c:623-696
  *                      (local score of the edges incident to a vertex set)
- *   orc_sweep / orc_triple_round  the best-per-row set commit that the engine
+ *   orc_quad_delta     4-set permutations: calculate_permutation_delta
+ *                      differences (src/permutation.c:623-744) for k = 4
+ *   orc_sweep / orc_triple_round / orc_quad_round  the best-per-row set commit that the engine
  *                      runs (candidates sorted by delta desc then ids, each
  *                      re-verified on the updated mapping).
  * Graph semantics match the reference loaders: every G1 edge entry counts,
@@ -421,6 +423,122 @@ int orc_triple_round(void* p, int* map, int partners, uint64_t seed, int max_can
         total += d;
         committed++;
         taint_nbrs(g, a, taint); taint_nbrs(g, b, taint); taint_nbrs(g, c, taint);
+    }
+    if (stats) {
+        stats[0] = total; stats[1] = nk; stats[2] = scanned; stats[3] = verified;
+        stats[4] = committed; stats[5] = nk ? (long long)(0x7fffffffu - (unsigned)(keys[0] >> 32)) : 0;
+        stats[6] = valid;
+    }
+    free(keys); free(used); free(taint);
+    return committed;
+}
+
+/* ---- 4-set permutations ----
+ * The k = 4 case of src/permutation.c:700-744 (generate_permutations over
+ * the images of a 4-vertex set, scored with calculate_permutation_delta
+ * :623-696), on sampled connected 4-sets and with the same best-per-vertex
+ * set commit as the 3-cycle round.  Permutation index q in 1..23 is the q-th
+ * permutation of (0,1,2,3) in lexicographic order (0 = identity): vertex i of
+ * the set takes the image of vertex perm[q][i]. */
+static const int kQuadPerm[24][4] = {
+    {0,1,2,3},{0,1,3,2},{0,2,1,3},{0,2,3,1},{0,3,1,2},{0,3,2,1},
+    {1,0,2,3},{1,0,3,2},{1,2,0,3},{1,2,3,0},{1,3,0,2},{1,3,2,0},
+    {2,0,1,3},{2,0,3,1},{2,1,0,3},{2,1,3,0},{2,3,0,1},{2,3,1,0},
+    {3,0,1,2},{3,0,2,1},{3,1,0,2},{3,1,2,0},{3,2,0,1},{3,2,1,0}};
+
+static void permute4(int* map, const int* set, int q) {
+    int f[4];
+    for (int i = 0; i < 4; i++) f[i] = map[set[i]];
+    for (int i = 0; i < 4; i++) map[set[i]] = f[kQuadPerm[q][i]];
+}
+
+int orc_quad_delta(void* p, const int* map, int a, int b, int c, int d, int q) {
+    const orc* g = (const orc*)p;
+    int set[4] = {a, b, c, d};
+    int* m2 = (int*)malloc(sizeof(int) * (g->n + 1));
+    memcpy(m2, map, sizeof(int) * (g->n + 1));
+    long long before = orc_local_score(p, map, set, 4);
+    permute4(m2, set, q);
+    long long after = orc_local_score(p, m2, set, 4);
+    free(m2);
+    return (int)(after - before);
+}
+
+/* 3-step walk of slot j of vertex a along undirected G1 edges: a -> b -> c
+ * -> d with h1 = mix64(seed ^ (a-1 << 32 | j)), h2 = mix64(h1), h3 =
+ * mix64(h2); valid when the four vertices are distinct. */
+int orc_sample_quad(void* p, uint64_t seed, int a, int j, int* b, int* c, int* d) {
+    const orc* g = (const orc*)p;
+    int da = ndeg(g, a);
+    if (da == 0) return 0;
+    uint64_t h1 = mix64(seed ^ (((uint64_t)(a - 1) << 32) | (unsigned)j));
+    *b = nbr_at(g, a, (int)(h1 % (uint64_t)da));
+    int db = ndeg(g, *b);
+    if (db == 0) return 0;
+    uint64_t h2 = mix64(h1);
+    *c = nbr_at(g, *b, (int)(h2 % (uint64_t)db));
+    int dc = ndeg(g, *c);
+    if (dc == 0) return 0;
+    uint64_t h3 = mix64(h2);
+    *d = nbr_at(g, *c, (int)(h3 % (uint64_t)dc));
+    return *b != a && *c != a && *c != *b && *d != a && *d != *b && *d != *c;
+}
+
+/* One 4-set round.  Keys (0x7fffffff - delta) << 32 | (a-1) << 16 | j << 5 | q;
+ * stats[0..6] = total delta, candidates, scanned, verified, committed, best
+ * delta, valid 4-sets. */
+int orc_quad_round(void* p, int* map, int partners, uint64_t seed, int max_candidates,
+                   int max_verify, long long* stats) {
+    const orc* g = (const orc*)p;
+    const int n = g->n;
+    uint64_t* keys = (uint64_t*)malloc(sizeof(uint64_t) * (n + 1));
+    long long valid = 0;
+    #pragma omp parallel for schedule(dynamic, 4) reduction(+:valid)
+    for (int a = 1; a <= n; a++) {
+        uint64_t k = ~0ULL;
+        for (int j = 0; j < partners; j++) {
+            int b, c, d;
+            if (!orc_sample_quad(p, seed, a, j, &b, &c, &d)) continue;
+            valid++;
+            for (int q = 1; q < 24; q++) {
+                int dd = orc_quad_delta(p, map, a, b, c, d, q);
+                if (dd > 0) {
+                    uint64_t kk = ((uint64_t)(0x7fffffffu - (unsigned)dd) << 32) |
+                                  ((uint64_t)(a - 1) << 16) | ((unsigned)j << 5) | (unsigned)q;
+                    if (kk < k) k = kk;
+                }
+            }
+        }
+        keys[a - 1] = k;
+    }
+    qsort(keys, n, sizeof(uint64_t), cmp_u64);
+    int nk = 0;
+    while (nk < n && keys[nk] != ~0ULL) nk++;
+    unsigned char* used = calloc(n + 1, 1);
+    unsigned char* taint = calloc(n + 1, 1);
+    long long total = 0;
+    int scanned = 0, verified = 0, committed = 0;
+    int lim = (max_candidates > 0 && max_candidates < nk) ? max_candidates : nk;
+    for (int k = 0; k < lim; k++) {
+        int a = (int)((keys[k] >> 16) & 0xffff) + 1, j = (int)((keys[k] >> 5) & 0x7ff), q = (int)(keys[k] & 31);
+        int d0 = (int)(0x7fffffffu - (unsigned)(keys[k] >> 32));
+        int b = 0, c = 0, d = 0;
+        orc_sample_quad(p, seed, a, j, &b, &c, &d);
+        scanned++;
+        if (used[a] || used[b] || used[c] || used[d]) continue;
+        int dd = d0;
+        if (taint[a] || taint[b] || taint[c] || taint[d]) {
+            if (max_verify >= 0 && verified >= max_verify) continue;
+            verified++;
+            dd = orc_quad_delta(p, map, a, b, c, d, q);
+        }
+        if (dd <= 0) continue;
+        int set[4] = {a, b, c, d};
+        permute4(map, set, q);
+        used[a] = used[b] = used[c] = used[d] = 1;
+        total += dd;
+        committed++;
+        taint_nbrs(g, a, taint); taint_nbrs(g, b, taint); taint_nbrs(g, c, taint); taint_nbrs(g, d, taint);
     }
     if (stats) {
         stats[0] = total; stats[1] = nk; stats[2] = scanned; stats[3] = verified;

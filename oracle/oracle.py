@@ -49,6 +49,9 @@ def orc_lib():
         L.orc_triple_delta.argtypes = [vp, vp, i32, i32, i32, i32]
         L.orc_sample_triple.argtypes = [vp, u64, i32, i32, C.POINTER(i32), C.POINTER(i32)]
         L.orc_triple_round.argtypes = [vp, vp, i32, u64, i32, i32, vp]
+        L.orc_quad_delta.argtypes = [vp, vp, i32, i32, i32, i32, i32]
+        L.orc_sample_quad.argtypes = [vp, u64, i32, i32, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)]
+        L.orc_quad_round.argtypes = [vp, vp, i32, u64, i32, i32, vp]
         _orc = L
     return _orc
 
@@ -122,6 +125,23 @@ class Oracle:
         orc_lib().orc_triple_round(self.h, _p(m), partners, seed, max_candidates, max_verify, _p(st))
         return dict(total_delta=int(st[0]), candidates=int(st[1]), scanned=int(st[2]), verified=int(st[3]),
                     committed=int(st[4]), best_delta=int(st[5]), triples=int(st[6]))
+
+    def quad_delta(self, m, a, b, c, d, q):
+        """Exact delta of permutation q (1..23) of the 4-set (a, b, c, d), 1-based."""
+        m = np.ascontiguousarray(m, np.int32)
+        return orc_lib().orc_quad_delta(self.h, _p(m), a, b, c, d, q)
+
+    def sample_quad(self, seed, a, j):
+        b, c, d = C.c_int32(), C.c_int32(), C.c_int32()
+        ok = orc_lib().orc_sample_quad(self.h, seed, a, j, C.byref(b), C.byref(c), C.byref(d))
+        return (b.value, c.value, d.value) if ok else None
+
+    def quad_round(self, m, partners=64, seed=0, max_candidates=0, max_verify=-1):
+        """Runs one 4-set round IN PLACE on m; returns stats dict."""
+        st = np.zeros(8, np.int64)
+        orc_lib().orc_quad_round(self.h, _p(m), partners, seed, max_candidates, max_verify, _p(st))
+        return dict(total_delta=int(st[0]), candidates=int(st[1]), scanned=int(st[2]), verified=int(st[3]),
+                    committed=int(st[4]), best_delta=int(st[5]), quads=int(st[6]))
 
 
 class RefGAO:

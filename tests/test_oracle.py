@@ -79,3 +79,56 @@ def test_oracle_first_improvement_terminates():
     assert c > 0
     # at the fixed point no swap improves
     assert (O.all_deltas(m) <= 0).all()
+
+
+def _permute4(m, s, q):
+    import itertools
+    perm = list(itertools.permutations(range(4)))[q]
+    m2 = m.copy()
+    for i in range(4):
+        m2[s[i]] = m[s[perm[i]]]
+    return m2
+
+
+def test_quad_delta_matches_reference_permutation_score(cfg0):
+    """4-set permutations: the oracle's delta equals the difference of the
+    reference's calculate_permutation_delta local score (src/permutation.c)
+    before and after permuting the images, for sampled connected 4-sets and
+    all 23 permutations."""
+    try:
+        R = oracle.RefPerm()
+    except OSError:
+        pytest.skip("reference not compiled on this machine")
+    g = cfg0
+    O = oracle.Oracle.from_pair(g)
+    gm = R.graph(g["src1"], g["dst1"], g["w1"])
+    gf = R.graph(g["src2"], g["dst2"], g["w2"])
+    m = g["map0"]
+    done = 0
+    for a in range(1, 200, 7):
+        for j in range(3):
+            s = O.sample_quad(11, a, j)
+            if s is None:
+                continue
+            st = [a, *s]
+            assert len(set(st)) == 4
+            before = R.local_score(gm, gf, m, st)
+            for q in range(1, 24):
+                ref = R.local_score(gm, gf, _permute4(m, st, q), st) - before
+                assert O.quad_delta(m, a, s[0], s[1], s[2], q) == ref
+            done += 1
+    assert done > 40
+
+
+def test_oracle_quad_round_rule(cfg0):
+    g = cfg0
+    O = oracle.Oracle.from_pair(g)
+    m = g["map0"].copy()
+    s = O.score(m)
+    for r in range(2):
+        st = O.quad_round(m, partners=16, seed=r)
+        assert st["committed"] > 0 and st["quads"] > 0
+        s2 = O.score(m)
+        assert s2 == s + st["total_delta"]
+        assert sorted(m[1:]) == list(range(1, g["n"] + 1))
+        s = s2
