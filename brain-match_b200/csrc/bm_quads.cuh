@@ -144,6 +144,71 @@ __global__ void k_quad_deltas(DevView<W16> g, const int* __restrict__ sets, cons
     }
 }
 
+// Best improving permutation of the set M (largest delta, then smallest q;
+// q = 0 and delta 0 if none improves).  Every value the 23 permutations need
+// is loaded once: the 4x4 block of S among the set's vertices, the 4x4 block
+// of W2 among their current images, and the set's internal G1 edges (up to
+// kQuadMaxInternal entries; a set with more falls back to quad_delta_S per
+// permutation, with the same result).
+constexpr int kQuadMaxInternal = 12;
+template <bool W16>
+__device__ void quad_best(const DevView<W16>& g, const unsigned* __restrict__ adj, int words, const int* M,
+                          const int* pm, int& best_d, int& best_q) {
+    typedef Ent<W16> EN;
+    const int n = g.n;
+    best_d = 0;
+    best_q = 0;
+    int ie_ij[kQuadMaxInternal], ie_w[kQuadMaxInternal];  // (i << 2 | j), weight
+    int ne = 0;
+    bool overflow = false;
+    for (int i = 0; i < 4 && !overflow; i++)
+        for (int j = 0; j < 4 && !overflow; j++) {
+            if (i == j || !adj_bit(adj, words, M[i], M[j])) continue;
+            for (int e = lower_bound_out(g, M[i], M[j]); e < g.off1o[M[i] + 1]; e++) {
+                const typename EN::T en = g.ent1o[e];
+                if (EN::id(en) != M[j]) break;
+                if (ne == kQuadMaxInternal) { overflow = true; break; }
+                ie_ij[ne] = (i << 2) | j;
+                ie_w[ne] = EN::w(en);
+                ne++;
+            }
+        }
+    if (overflow) {
+        for (int q = 1; q < 24; q++) {
+            const int dd = quad_delta_S<W16>(g, adj, words, M, pm, q);
+            if (dd > best_d) { best_d = dd; best_q = q; }
+        }
+        return;
+    }
+    int sm[4][4], wm[4][4];  // S[M_i][M_j]; W2[p M_i][p M_j]
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            sm[i][j] = g.S[(size_t)M[i] * n + M[j]];
+            wm[i][j] = g.w2(pm[i], pm[j]);
+        }
+    for (int q = 1; q < 24; q++) {
+        int sg[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) sg[i] = kQuadPerm[q][i];
+        int d = 0;
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+            if (sg[i] != i) d += sm[i][sg[i]] - sm[i][i];
+        for (int t = 0; t < ne; t++) {
+            const int i = ie_ij[t] >> 2, j = ie_ij[t] & 3, w = ie_w[t];
+            if (sg[i] == j)
+                d -= imin(w, wm[i][j]) + imin(w, wm[j][i]) - imin(w, wm[i][i]) - imin(w, wm[j][j]);
+            int counted = 0;
+            if (sg[i] != i) counted += imin(w, wm[sg[i]][j]) - imin(w, wm[i][j]);
+            if (sg[j] != j) counted += imin(w, wm[i][sg[j]]) - imin(w, wm[i][j]);
+            d += imin(w, wm[sg[i]][sg[j]]) - imin(w, wm[i][j]) - counted;
+        }
+        if (d > best_d) { best_d = d; best_q = q; }
+    }
+}
+
 // Sample `partners` 4-sets per vertex a, evaluate the 23 permutations of each
 // from S, keep per vertex the best improving one as a sort key
 //   (0x7fffffff - delta) << 32 | a << 16 | slot << 5 | q     (~0 if none)
@@ -163,13 +228,12 @@ k_quad_eval(DevView<W16> g, const unsigned* __restrict__ adj, int words, int par
             valid++;
             const int M[4] = {a, b, c, d};
             const int pm[4] = {g.p[a], g.p[b], g.p[c], g.p[d]};
-            for (int q = 1; q < 24; q++) {
-                const int dd = quad_delta_S<W16>(g, adj, words, M, pm, q);
-                if (dd > 0) {
-                    const unsigned long long kk = ((unsigned long long)(0x7fffffffu - (unsigned)dd) << 32) |
-                                                  ((unsigned long long)a << 16) | ((unsigned)j << 5) | (unsigned)q;
-                    if (kk < k) k = kk;
-                }
+            int dd, q;
+            quad_best<W16>(g, adj, words, M, pm, dd, q);
+            if (dd > 0) {
+                const unsigned long long kk = ((unsigned long long)(0x7fffffffu - (unsigned)dd) << 32) |
+                                              ((unsigned long long)a << 16) | ((unsigned)j << 5) | (unsigned)q;
+                if (kk < k) k = kk;
             }
         }
         for (int o = 16; o; o >>= 1) {
