@@ -304,10 +304,11 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
                 s_corr[lane] = 0; s_cnt[lane] = 0; s_imask[lane] = 0;
                 atomicOr_u16(&mark[a], (uint16_t)(1u << lane));
                 atomicOr_u16(&mark[b], (uint16_t)(1u << lane));
-                unsigned sh = 0;
-                for (int i = 0; i < lane; i++)
-                    if (a == s_lo[i] || a == s_hi[i] || b == s_lo[i] || b == s_hi[i]) sh |= 1u << i;
-                s_share[lane] = sh;
+            }
+            __syncwarp();
+            if (lane < cnt) {  // earlier pairs of the step that share a vertex: read off the marks
+                const unsigned m = (unsigned)mark[s_lo[lane]] | (unsigned)mark[s_hi[lane]];
+                s_share[lane] = m & ((1u << lane) - 1u);
             }
             int incl = len;  // inclusive prefix over lanes
             for (int o = 1; o < 32; o <<= 1) {
