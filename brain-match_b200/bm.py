@@ -34,13 +34,13 @@ class Info(C.Structure):
 
 class SweepOpts(C.Structure):
     _fields_ = [("max_candidates", C.c_int32), ("max_verify", C.c_int32), ("commit_ctas", C.c_int32),
-                ("reserved", C.c_int32 * 5)]
+                ("incremental", C.c_int32), ("reserved", C.c_int32 * 4)]
 
 
 class SweepStats(C.Structure):
     _fields_ = [("score_before", C.c_int64), ("score_after", C.c_int64), ("deltas_evaluated", C.c_int64),
                 ("candidates", C.c_int32), ("scanned", C.c_int32), ("verified", C.c_int32),
-                ("committed", C.c_int32), ("best_delta", C.c_int32), ("reserved", C.c_int32),
+                ("committed", C.c_int32), ("best_delta", C.c_int32), ("profit_mode", C.c_int32),
                 ("ms_profit", C.c_float), ("ms_combine", C.c_float), ("ms_commit", C.c_float),
                 ("ms_total", C.c_float), ("ms_prep", C.c_float), ("ms_hub", C.c_float), ("min_terms", C.c_int64),
                 ("commit_entries", C.c_int64), ("commit_steps", C.c_int32), ("commit_carried", C.c_int32)]
@@ -57,6 +57,12 @@ class TripleStats(C.Structure):
                 ("verified", C.c_int32), ("committed", C.c_int32), ("best_delta", C.c_int32),
                 ("reserved", C.c_int32), ("ms_sample", C.c_float), ("ms_eval", C.c_float),
                 ("ms_commit", C.c_float), ("ms_total", C.c_float)]
+
+
+class LookupStats(C.Structure):
+    _fields_ = [("score_before", C.c_int64), ("score_after", C.c_int64), ("swaps", C.c_int32),
+                ("converged", C.c_int32), ("refresh_mode", C.c_int32), ("reserved", C.c_int32),
+                ("ms_refresh", C.c_float), ("ms_total", C.c_float)]
 
 
 class MlpTrainStats(C.Structure):
@@ -120,6 +126,8 @@ def lib():
         L.bm_first_improvement.argtypes = [vp, i32, C.POINTER(i64), C.POINTER(i32)]
         L.bm_triple_deltas.argtypes = [vp, i64, vp, vp, vp, vp]
         L.bm_triple_round.argtypes = [vp, C.POINTER(TripleOpts), C.POINTER(TripleStats)]
+        L.bm_lookup_rows.argtypes = [vp, i32, i32, vp]
+        L.bm_lookup_descent.argtypes = [vp, i32, C.POINTER(LookupStats)]
         L.bm_timer_mark.argtypes = [vp, i32]
         L.bm_timer_elapsed.argtypes = [vp, i32, i32, C.POINTER(C.c_float)]
         L.bm_measure_peaks.argtypes = [i32, C.POINTER(C.c_double), C.POINTER(C.c_double)]
@@ -284,11 +292,22 @@ class Engine:
         _check(lib().bm_profit_row(self.h, int(a), _p(out)), self.h)
         return out
 
-    def sweep(self, max_candidates=0, max_verify=-1, commit_ctas=0):
-        o = SweepOpts(max_candidates, max_verify, commit_ctas)
+    def sweep(self, max_candidates=0, max_verify=-1, commit_ctas=0, incremental=False):
+        o = SweepOpts(max_candidates, max_verify, commit_ctas, int(bool(incremental)))
         s = SweepStats()
         _check(lib().bm_sweep(self.h, C.byref(o), C.byref(s)), self.h)
         return {k: getattr(s, k) for k, _ in SweepStats._fields_ if k != "reserved"}
+
+    def lookup_rows(self, a0, rows):
+        """Rows a0..a0+rows-1 (1-based) of the exact delta table, shape [rows, n]."""
+        out = np.zeros((int(rows), self.n), np.int32)
+        _check(lib().bm_lookup_rows(self.h, int(a0), int(rows), _p(out)), self.h)
+        return out
+
+    def lookup_descent(self, max_swaps):
+        s = LookupStats()
+        _check(lib().bm_lookup_descent(self.h, int(max_swaps), C.byref(s)), self.h)
+        return {k: getattr(s, k) for k, _ in LookupStats._fields_ if k != "reserved"}
 
     def timer_mark(self, slot):
         _check(lib().bm_timer_mark(self.h, slot), self.h)

@@ -20,6 +20,7 @@
 #include "bm_quads.cuh"
 #include "bm_select.cuh"
 #include "bm_hub.cuh"
+#include "bm_incr.cuh"
 
 using namespace bm;
 
@@ -146,6 +147,8 @@ static void free_ctx(bm_ctx* c) {
         if (b) cudaFree(b);
     if (c->cinfo) cudaFree(c->cinfo);
     if (c->cgrid) cudaFree(c->cgrid);
+    for (void* b : {(void*)c->pS, (void*)c->pinvS, (void*)c->moved, (void*)c->minfo, (void*)c->mwork})
+        if (b) cudaFree(b);
     if (c->ev_hub) cudaEventDestroy(c->ev_hub);
     if (c->st) cudaStreamDestroy(c->st);
     delete c;
@@ -235,6 +238,8 @@ extern "C" bm_status bm_create(bm_ctx** out, int32_t n, int64_t e1, const int32_
     ctx->e1 = (long long)s1.size();
     ctx->e2 = (long long)s2.size();
     ctx->nself = (long long)selfv.size();
+    for (int v = 0; v < n; v++)
+        ctx->max_deg1 = std::max(ctx->max_deg1, (g1o.off[v + 1] - g1o.off[v]) + (g1i.off[v + 1] - g1i.off[v]));
     auto fail = [&](bm_status s) {
         snprintf(g_create_err, sizeof g_create_err, "%s", ctx->err);
         free_ctx(ctx);
@@ -465,6 +470,18 @@ extern "C" bm_status bm_pair_deltas(bm_ctx* ctx, int64_t k, const int32_t* m1, c
 
 // ---------------------------------------------------------------------------
 // Sweep stages.
+// S is now exact for the current matching: remember which one.
+static cudaError_t record_exact_mapping(bm_ctx* ctx) {
+    const size_t bytes = (size_t)(ctx->n + 1) * sizeof(int);
+    cudaError_t e = cudaSuccess;
+    if (!ctx->pS) e = dalloc(ctx, &ctx->pS, bytes);
+    if (e == cudaSuccess && !ctx->pinvS) e = dalloc(ctx, &ctx->pinvS, bytes);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->pS, ctx->p, bytes, cudaMemcpyDeviceToDevice, ctx->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->pinvS, ctx->pinv, bytes, cudaMemcpyDeviceToDevice, ctx->st);
+    ctx->S_exact = e == cudaSuccess;
+    return e;
+}
+
 bm_status ensure_S(bm_ctx* ctx) {
     if (ctx->S) return BM_OK;
     CK(dalloc(ctx, &ctx->S, (size_t)ctx->n * ctx->n * sizeof(int)));
@@ -476,6 +493,7 @@ bm_status stage_profit(bm_ctx* ctx) {
     typedef typename Ent<W16>::T E;
     DevView<W16> g = view<W16>(ctx);
     const int n = ctx->n;
+    ctx->S_exact = false;
     const int rb = ctx->num_sms * 8;
     k_relabel<W16><<<rb, 256, 0, ctx->st>>>((const E*)ctx->ent1o, (E*)ctx->ent1oP, ctx->e1, ctx->p);
     k_relabel<W16><<<rb, 256, 0, ctx->st>>>((const E*)ctx->ent1i, (E*)ctx->ent1iP, ctx->e1, ctx->p);
@@ -519,12 +537,80 @@ bm_status stage_profit(bm_ctx* ctx) {
     k_profit<W16><<<ctx->num_sms * per_sm, 512, smem, ctx->st>>>(g, ctx->order, ctx->small,
                                                                 ctx->nh ? ctx->is_hub : nullptr, kHubT);
     CK(cudaGetLastError());
+    CK(record_exact_mapping(ctx));
     CK(cudaEventRecord(ctx->ev[5], ctx->st));
     return BM_OK;
 }
 
 template bm_status stage_profit<true>(bm_ctx*);
 template bm_status stage_profit<false>(bm_ctx*);
+
+template <bool W16>
+bm_status stage_refresh(bm_ctx* ctx, int* mode) {
+    *mode = 0;
+    if (!ctx->S_exact) return stage_profit<W16>(ctx);
+    const int n = ctx->n;
+    if (!ctx->moved) {
+        CK(dalloc(ctx, &ctx->moved, (size_t)n * sizeof(int)));
+        CK(dalloc(ctx, &ctx->minfo, 4 * sizeof(int)));
+        CK(dalloc(ctx, &ctx->mwork, sizeof(unsigned long long)));
+    }
+    DevView<W16> g = view<W16>(ctx);
+    CK(cudaMemsetAsync(ctx->minfo, 0, 4 * sizeof(int), ctx->st));
+    CK(cudaMemsetAsync(ctx->mwork, 0, sizeof(unsigned long long), ctx->st));
+    k_moved<W16><<<ctx->num_sms * 2, 256, 0, ctx->st>>>(g, ctx->pS, ctx->pinvS, ctx->moved, ctx->minfo, ctx->mwork);
+    CK(cudaGetLastError());
+    int info[4];
+    unsigned long long work = 0, full = 0;
+    CK(cudaMemcpyAsync(info, ctx->minfo, sizeof info, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(&work, ctx->mwork, sizeof work, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(&full, ctx->work_sum, sizeof full, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    CK(cudaEventRecord(ctx->ev_hub, ctx->st));
+    CK(cudaEventRecord(ctx->ev[4], ctx->st));
+    const int count = info[0];
+    ctx->upd_work = (long long)work;
+    if (count == 0) {
+        *mode = 2;
+        CK(cudaEventRecord(ctx->ev[5], ctx->st));
+        return BM_OK;
+    }
+    // an atomic into S costs about kIncrAtomicCost shared-memory terms of a
+    // rebuild, a permuted column entry kIncrPermCost
+    const double est = kIncrAtomicCost * (double)work + kIncrPermCost * (double)n * count;
+    if (info[1] || count > kIncrMaxMoved || est >= (double)full) return stage_profit<W16>(ctx);
+    const int maxd = std::max(info[2], 1);
+    ctx->S_exact = false;
+    {
+        dim3 grid(count, (maxd + kIncrCornerEdges - 1) / kIncrCornerEdges);
+        k_corner<W16><<<grid, kIncrCornerEdges, 0, ctx->st>>>(g, ctx->pS, ctx->pS, ctx->moved, count, nullptr, -1);
+        CK(cudaGetLastError());
+    }
+    {
+        const size_t smem = 3 * (size_t)count * sizeof(int);
+        CK(cudaFuncSetAttribute(k_perm_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        const int blocks = std::min(n, ctx->num_sms * (smem <= 48 * 1024 ? 4 : 1));
+        k_perm_cols<<<blocks, 512, smem, ctx->st>>>(ctx->S, n, ctx->moved, count, ctx->p, ctx->pinvS);
+        CK(cudaGetLastError());
+    }
+    {
+        dim3 grid(count, (maxd + kIncrEdgesPerBlock - 1) / kIncrEdgesPerBlock);
+        k_terms<W16><<<grid, 256, 0, ctx->st>>>(g, ctx->pS, ctx->moved, count, nullptr);
+        CK(cudaGetLastError());
+    }
+    {
+        dim3 grid(count, (maxd + kIncrCornerEdges - 1) / kIncrCornerEdges);
+        k_corner<W16><<<grid, kIncrCornerEdges, 0, ctx->st>>>(g, ctx->p, ctx->pS, ctx->moved, count, nullptr, 1);
+        CK(cudaGetLastError());
+    }
+    CK(record_exact_mapping(ctx));
+    CK(cudaEventRecord(ctx->ev[5], ctx->st));
+    *mode = 1;
+    return BM_OK;
+}
+
+template bm_status stage_refresh<true>(bm_ctx*, int*);
+template bm_status stage_refresh<false>(bm_ctx*, int*);
 
 bm_status stage_combine(bm_ctx* ctx, int* all_out) {
     const int n = ctx->n;
@@ -630,7 +716,11 @@ extern "C" bm_status bm_sweep(bm_ctx* ctx, const bm_sweep_opts* opts, bm_sweep_s
     if (s) return s;
     const long long before = ctx->score;
     CK(cudaEventRecord(ctx->ev[0], ctx->st));
-    s = ctx->w16 ? stage_profit<true>(ctx) : stage_profit<false>(ctx);
+    int mode = 0;
+    if (opts && opts->incremental)
+        s = ctx->w16 ? stage_refresh<true>(ctx, &mode) : stage_refresh<false>(ctx, &mode);
+    else
+        s = ctx->w16 ? stage_profit<true>(ctx) : stage_profit<false>(ctx);
     if (s) return s;
     CK(cudaEventRecord(ctx->ev[1], ctx->st));
     s = stage_combine(ctx, nullptr);
@@ -660,6 +750,7 @@ extern "C" bm_status bm_sweep(bm_ctx* ctx, const bm_sweep_opts* opts, bm_sweep_s
         stats->deltas_evaluated = (long long)ctx->n * (ctx->n - 1) / 2;
         stats->candidates = small[1];
         stats->best_delta = small[2];
+        stats->profit_mode = mode;
         stats->scanned = cs.scanned;
         stats->verified = cs.verified;
         stats->committed = cs.committed;
@@ -669,12 +760,110 @@ extern "C" bm_status bm_sweep(bm_ctx* ctx, const bm_sweep_opts* opts, bm_sweep_s
         cudaEventElapsedTime(&stats->ms_combine, ctx->ev[1], ctx->ev[2]);
         cudaEventElapsedTime(&stats->ms_commit, ctx->ev[2], ctx->ev[3]);
         cudaEventElapsedTime(&stats->ms_total, ctx->ev[0], ctx->ev[3]);
-        stats->min_terms = (long long)terms;
+        stats->min_terms = mode == 1 ? ctx->upd_work : mode == 2 ? 0 : (long long)terms;
         stats->commit_entries = cs.entries;
         stats->commit_steps = cs.steps;
         stats->commit_carried = cs.carried;
     }
     return BM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Exact swap-lookup table (src/best-swap/create-score-lookup.c:289-296,
+// src/best-swap/score-lookup.c:514-640): the table is the profit matrix, kept
+// exact by the moved-vertex update; the heap is the per-row best partners.
+static bm_status ensure_moved(bm_ctx* ctx) {
+    if (ctx->moved) return BM_OK;
+    CK(dalloc(ctx, &ctx->moved, (size_t)ctx->n * sizeof(int)));
+    CK(dalloc(ctx, &ctx->minfo, 4 * sizeof(int)));
+    CK(dalloc(ctx, &ctx->mwork, sizeof(unsigned long long)));
+    return BM_OK;
+}
+
+extern "C" bm_status bm_lookup_rows(bm_ctx* ctx, int32_t a0, int32_t rows, int32_t* out) {
+    if (!ctx || !out || rows < 0) return BM_E_INPUT;
+    if (!ctx->mapped) { set_err(ctx, "bm_lookup_rows: no mapping set"); return BM_E_STATE; }
+    if (a0 < 1 || (long long)a0 + rows - 1 > ctx->n) {
+        set_err(ctx, "bm_lookup_rows: rows %d..%lld outside 1..%d", a0, (long long)a0 + rows - 1, ctx->n);
+        return BM_E_INPUT;
+    }
+    if (rows == 0) return BM_OK;
+    bm_status s = ensure_S(ctx);
+    if (s) return s;
+    int mode = 0;
+    s = ctx->w16 ? stage_refresh<true>(ctx, &mode) : stage_refresh<false>(ctx, &mode);
+    if (s) return s;
+    const long long total = (long long)rows * ctx->n;
+    if ((s = ensure_scratch(ctx, total))) return s;
+    k_delta_rows<<<ctx->num_sms * 8, 256, 0, ctx->st>>>(ctx->S, ctx->n, a0 - 1, rows, ctx->scratch_pairs);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, ctx->scratch_pairs, total * sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return BM_OK;
+}
+
+template <bool W16>
+static bm_status lookup_descent_impl(bm_ctx* ctx, int max_swaps, bm_lookup_stats* st) {
+    const int n = ctx->n;
+    bm_status s = ensure_S(ctx);
+    if (!s) s = ensure_moved(ctx);
+    if (s) return s;
+    if (!ctx->fi_acc) CK(dalloc(ctx, &ctx->fi_acc, 2 * sizeof(long long)));
+    const long long before = ctx->score;
+    CK(cudaEventRecord(ctx->ev[0], ctx->st));
+    int mode = 0;
+    s = stage_refresh<W16>(ctx, &mode);
+    if (s) return s;
+    CK(cudaEventRecord(ctx->ev[1], ctx->st));
+    CK(cudaMemsetAsync(ctx->minfo, 0, 4 * sizeof(int), ctx->st));
+    CK(cudaMemsetAsync(ctx->fi_acc, 0, 2 * sizeof(long long), ctx->st));
+    DevView<W16> g = view<W16>(ctx);
+    const int maxd = std::max(ctx->max_deg1, 1);
+    const dim3 gc(2, (maxd + kIncrCornerEdges - 1) / kIncrCornerEdges);
+    const dim3 gt(2, (maxd + kIncrEdgesPerBlock - 1) / kIncrEdgesPerBlock);
+    const int pblocks = std::max(1, std::min((n + 255) / 256, ctx->num_sms * 4));
+    int info[4] = {0, 0, 0, 0};
+    long long acc[2] = {0, 0};
+    int done = 0;
+    while (done < max_swaps && !info[3]) {
+        const int batch = std::min(kLookupBatch, max_swaps - done);
+        for (int k = 0; k < batch; k++) {
+            s = stage_combine(ctx, nullptr);
+            if (s) return s;
+            k_pick_commit<<<1, 1024, 0, ctx->st>>>(ctx->rowbest, n, ctx->p, ctx->pinv, ctx->moved, ctx->minfo,
+                                                   ctx->fi_acc);
+            k_corner<W16><<<gc, kIncrCornerEdges, 0, ctx->st>>>(g, ctx->pS, ctx->pS, ctx->moved, 2, ctx->minfo, -1);
+            k_perm_cols_small<<<pblocks, 256, 0, ctx->st>>>(ctx->S, n, ctx->moved, ctx->minfo, ctx->p, ctx->pinvS);
+            k_terms<W16><<<gt, 256, 0, ctx->st>>>(g, ctx->pS, ctx->moved, 2, ctx->minfo);
+            k_corner<W16><<<gc, kIncrCornerEdges, 0, ctx->st>>>(g, ctx->p, ctx->pS, ctx->moved, 2, ctx->minfo, 1);
+            k_sync_exact<<<1, 32, 0, ctx->st>>>(ctx->moved, ctx->minfo, ctx->p, ctx->pS, ctx->pinvS, n);
+            CK(cudaGetLastError());
+        }
+        done += batch;
+        CK(cudaMemcpyAsync(info, ctx->minfo, sizeof info, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaMemcpyAsync(acc, ctx->fi_acc, sizeof acc, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+    }
+    CK(cudaEventRecord(ctx->ev[2], ctx->st));
+    CK(cudaEventSynchronize(ctx->ev[2]));
+    ctx->score = before + acc[0];
+    if (st) {
+        memset(st, 0, sizeof *st);
+        st->score_before = before;
+        st->score_after = ctx->score;
+        st->swaps = (int32_t)acc[1];
+        st->converged = info[3] ? 1 : 0;
+        st->refresh_mode = mode;
+        cudaEventElapsedTime(&st->ms_refresh, ctx->ev[0], ctx->ev[1]);
+        cudaEventElapsedTime(&st->ms_total, ctx->ev[0], ctx->ev[2]);
+    }
+    return BM_OK;
+}
+
+extern "C" bm_status bm_lookup_descent(bm_ctx* ctx, int32_t max_swaps, bm_lookup_stats* stats) {
+    if (!ctx || max_swaps < 0) return BM_E_INPUT;
+    if (!ctx->mapped) { set_err(ctx, "bm_lookup_descent: no mapping set"); return BM_E_STATE; }
+    return ctx->w16 ? lookup_descent_impl<true>(ctx, max_swaps, stats) : lookup_descent_impl<false>(ctx, max_swaps, stats);
 }
 
 extern "C" bm_status bm_timer_mark(bm_ctx* ctx, int32_t slot) {

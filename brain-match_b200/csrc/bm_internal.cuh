@@ -15,6 +15,7 @@ struct bm_ctx {
     int dev = 0, num_sms = 0;
     size_t smem_optin = 0;  // opt-in shared memory per block
     long long e1 = 0, e2 = 0, nself = 0;
+    int max_deg1 = 0;       // largest G1 degree (in + out, self-loops apart)
     cudaStream_t st = nullptr;
     char err[512] = {0};
     bool mapped = false;
@@ -42,6 +43,13 @@ struct bm_ctx {
     CommitStats* cstats = nullptr;
     int4* cinfo = nullptr;  // list extents of the sorted candidates (2 per candidate)
     int* cgrid = nullptr;   // set commit across CTAs: partial sums [2][32][8][3], barrier [2], error [1]
+    // S kept exact across commits: the matching it is exact for, and the moved-vertex update
+    bool S_exact = false;
+    int *pS = nullptr, *pinvS = nullptr;  // n+1 entries each
+    int* moved = nullptr;                 // moved vertices (n)
+    int* minfo = nullptr;                 // [0] count [1] needs rebuild [2] max degree
+    unsigned long long* mwork = nullptr;  // list entries the update touches
+    long long upd_work = 0;               // ... in the last update (host copy)
     int* scratch_pairs = nullptr;  // pair/triple inputs and outputs (ints)
     long long scratch_cap = 0;
     unsigned* adj = nullptr;       // G1 adjacency bitmap (3-cycles)
@@ -112,4 +120,8 @@ bm_status ensure_S(bm_ctx* ctx);
 // Sweep stages shared by the exhaustive and the learned sweep (bm_engine.cu):
 // the profit matrix S of the current matching, then each row's best partner.
 template <bool W16> bm_status stage_profit(bm_ctx* ctx);
+// S made exact for the current matching: an update from the vertices whose
+// image changed since S was last exact when that is cheaper, else
+// stage_profit.  *mode: 0 rebuilt, 1 updated, 2 already exact.
+template <bool W16> bm_status stage_refresh(bm_ctx* ctx, int* mode);
 bm_status stage_combine(bm_ctx* ctx, int* all_out);

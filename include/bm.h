@@ -169,7 +169,11 @@ typedef struct {
     int32_t commit_ctas;     /* CTAs (one thread-block cluster) sharing the set
                                 commit's list scans: 0 = default (8), 1..8;
                                 results never depend on it                      */
-    int32_t reserved[5];
+    int32_t incremental;     /* 1: keep the profit matrix exact across sweeps and
+                                update it from the vertices the last commit moved
+                                when that is cheaper than a rebuild; results never
+                                depend on it                                     */
+    int32_t reserved[4];
 } bm_sweep_opts;
 
 typedef struct {
@@ -181,7 +185,8 @@ typedef struct {
     int32_t verified;           /* tainted candidates re-evaluated       */
     int32_t committed;          /* swaps applied                         */
     int32_t best_delta;         /* largest delta of the sweep            */
-    int32_t reserved;
+    int32_t profit_mode;        /* 0 rebuilt, 1 updated from the moved
+                                   vertices, 2 already exact              */
     /* device time (CUDA events on the context's stream), milliseconds:      */
     float   ms_profit;          /* profit-row kernel alone                */
     float   ms_combine;         /* pair combine + per-row best            */
@@ -189,7 +194,8 @@ typedef struct {
     float   ms_total;           /* whole sweep                            */
     float   ms_prep;            /* relabelling + row scheduling           */
     float   ms_hub;             /* hub operands + tensor-core GEMM        */
-    int64_t min_terms;          /* nonzero min terms scattered            */
+    int64_t min_terms;          /* nonzero min terms scattered by a rebuild,
+                                   list entries applied by an update       */
     int64_t commit_entries;     /* edge-list entries read by the commit   */
     int32_t commit_steps;       /* commit steps (pairs decided per step)  */
     int32_t commit_carried;     /* pairs carried into a later step        */
@@ -238,6 +244,45 @@ bm_status bm_timer_elapsed(bm_ctx* ctx, int32_t start_slot, int32_t end_slot, fl
  * Allocates a 4-byte scratch word; diagnostic, not on the hot path.
  */
 bm_status bm_measure_peaks(int32_t n, double* red_per_s, double* minadd_per_s);
+
+/* ---- Exact swap-lookup table ----
+ * The reference's best-swap tools keep an n x n table of swap deltas
+ * (src/best-swap/create-score-lookup.c:289-296) and a heap of its positive
+ * entries; after each swap they recompute only the rows and columns of the
+ * two swapped vertices (src/best-swap/score-lookup.c:514-537), so every pair
+ * next to them goes stale.  Here the table is the context's profit matrix,
+ * kept exact across commits by the update of bm_sweep_opts.incremental (every
+ * term that the moved vertices change), and the heap is each row's best
+ * partner, recomputed from the exact table at every step. */
+
+/*
+ * Rows a0 .. a0+rows-1 (1-based) of the exact delta table on the current
+ * matching: out[(a-a0)*n + (b-1)] = delta of swapping map[a] and map[b],
+ * 0 for b == a.  The create-score-lookup table, row-chunked so a caller can
+ * stream n x n entries to a file.
+ */
+bm_status bm_lookup_rows(bm_ctx* ctx, int32_t a0, int32_t rows, int32_t* out);
+
+typedef struct {
+    int64_t score_before, score_after;
+    int32_t swaps;          /* swaps committed                               */
+    int32_t converged;      /* 1: stopped because no swap improves           */
+    int32_t refresh_mode;   /* how the table was made exact first: 0 rebuilt,
+                               1 updated, 2 already exact                     */
+    int32_t reserved;
+    float   ms_refresh;     /* device time of making the table exact        */
+    float   ms_total;       /* device time of the whole call                 */
+} bm_lookup_stats;
+
+/*
+ * Best-swap descent (the extract_max / swap / update loop of
+ * src/best-swap/score-lookup.c:597-640) on the exact table: each step commits
+ * the swap of largest delta over all pairs (ties: smallest first vertex, then
+ * smallest second) while it is > 0, then updates the table, up to max_swaps
+ * swaps.  Zero-delta and temperature-accepted swaps (:548-595) are not made:
+ * with an exact table a zero-delta swap is followed by its own reversal.
+ */
+bm_status bm_lookup_descent(bm_ctx* ctx, int32_t max_swaps, bm_lookup_stats* stats);
 
 /* ---- 3-cycles ---- */
 

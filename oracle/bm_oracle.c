@@ -14,6 +14,9 @@
  *                      (local score of the edges incident to a vertex set)
  *   orc_quad_delta     4-set permutations: calculate_permutation_delta
  *                      differences (src/permutation.c:623-744) for k = 4
+ *   orc_best_swap_descent  the extract_max / swap / update loop of the
+ *                      best-swap tool (src/best-swap/score-lookup.c:597-640)
+ *                      on an exact delta table, largest delta first
  *   orc_sweep / orc_triple_round / orc_quad_round  the best-per-row set commit that the engine
  *                      runs (candidates sorted by delta desc then ids, each
  *                      re-verified on the updated mapping).
@@ -547,4 +550,29 @@ int orc_quad_round(void* p, int* map, int partners, uint64_t seed, int max_candi
     }
     free(keys); free(used); free(taint);
     return committed;
+}
+
+/* Best-swap descent on an exact table (src/best-swap/score-lookup.c:597-640
+ * with every delta current): each step swaps the pair of largest delta over
+ * all pairs, the first in (m1, m2) order among equals, while that delta is
+ * > 0.  swaps[2i], swaps[2i+1] and deltas[i] record step i (either may be
+ * NULL).  Returns the number of swaps. */
+int orc_best_swap_descent(void* p, int* map, int max_swaps, int* swaps, int* deltas) {
+    const orc* g = (const orc*)p;
+    const int n = g->n;
+    int done = 0;
+    while (done < max_swaps) {
+        int bd = 0, ba = 0, bb = 0;
+        for (int a = 1; a <= n; a++)
+            for (int b = a + 1; b <= n; b++) {
+                const int d = orc_swap_delta(p, map, a, b);
+                if (d > bd) { bd = d; ba = a; bb = b; }
+            }
+        if (bd <= 0) break;
+        const int t = map[ba]; map[ba] = map[bb]; map[bb] = t;
+        if (swaps) { swaps[2 * done] = ba; swaps[2 * done + 1] = bb; }
+        if (deltas) deltas[done] = bd;
+        done++;
+    }
+    return done;
 }

@@ -52,6 +52,7 @@ def orc_lib():
         L.orc_quad_delta.argtypes = [vp, vp, i32, i32, i32, i32, i32]
         L.orc_sample_quad.argtypes = [vp, u64, i32, i32, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)]
         L.orc_quad_round.argtypes = [vp, vp, i32, u64, i32, i32, vp]
+        L.orc_best_swap_descent.argtypes = [vp, vp, i32, vp, vp]
         _orc = L
     return _orc
 
@@ -100,6 +101,13 @@ class Oracle:
         if want_moves:
             d["moves"] = mv[:3 * c].reshape(-1, 3)
         return d
+
+    def best_swap_descent(self, m, max_swaps):
+        """Best-swap descent IN PLACE on m; returns (pairs [k,2], deltas [k])."""
+        sw = np.zeros(2 * max(max_swaps, 1), np.int32)
+        dl = np.zeros(max(max_swaps, 1), np.int32)
+        k = orc_lib().orc_best_swap_descent(self.h, _p(m), int(max_swaps), _p(sw), _p(dl))
+        return sw[:2 * k].reshape(-1, 2), dl[:k]
 
     def first_improvement(self, m, max_passes):
         p, ds = i32(), i64()

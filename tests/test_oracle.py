@@ -81,6 +81,37 @@ def test_oracle_first_improvement_terminates():
     assert (O.all_deltas(m) <= 0).all()
 
 
+def test_oracle_best_swap_descent_against_reference_deltas():
+    """Each step of the best-swap descent takes the largest of the compiled
+    reference's deltas over all pairs (first in pair order among equals), and
+    the score moves by exactly that delta."""
+    try:
+        R = oracle.RefGAO()
+    except OSError:
+        pytest.skip("reference not compiled on this machine")
+    z = load_golden("small_n40")
+    O = _pair(z)
+    gm = R.graph(z["src1"], z["dst1"], z["w1"])
+    gf = R.graph(z["src2"], z["dst2"], z["w2"])
+    n = int(z["n"])
+    a, b = np.triu_indices(n, 1)
+    m = z["map0"].copy()
+    steps = 0
+    while True:
+        ref = R.pair_deltas(gm, gf, m, a + 1, b + 1)
+        mm = m.copy()
+        pairs, deltas = O.best_swap_descent(mm, 1)
+        if ref.max() <= 0:
+            assert len(deltas) == 0
+            break
+        i = int(np.argmax(ref))
+        assert (pairs[0, 0], pairs[0, 1], deltas[0]) == (a[i] + 1, b[i] + 1, ref[i])
+        assert O.score(mm) == O.score(m) + int(deltas[0]) == R.score(gm, gf, mm)
+        m = mm
+        steps += 1
+    assert steps > 5
+
+
 def _permute4(m, s, q):
     import itertools
     perm = list(itertools.permutations(range(4)))[q]
