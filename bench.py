@@ -269,6 +269,27 @@ def run_engine(args, g, world, rank, local, pg):
                       "note": "above 1 because the sparse profit matrix skips the zero min terms "
                               "that the per-pair formula counts"}
 
+    # descent to convergence from the initial matching, device time: sweeps
+    # that rebuild the profit matrix against sweeps that update it from the
+    # vertices the previous commit moved (identical moves, checked here)
+    descent = None
+    if not args.no_descent:
+        runs = {}
+        for inc in (False, True):
+            E.set_mapping(g["map0"])
+            tot, upd, sw = 0.0, 0, 0
+            for _ in range(500):
+                s = E.sweep(incremental=inc)
+                tot += s["ms_total"]
+                upd += s["profit_mode"] == 1
+                sw += 1
+                if s["committed"] == 0:
+                    break
+            runs[inc] = (tot, upd, sw, s["score_after"], E.get_mapping())
+        assert runs[False][3] == runs[True][3] and np.array_equal(runs[False][4], runs[True][4])
+        descent = {"sweeps": runs[False][2], "final_score": runs[False][3], "rebuild_ms": runs[False][0],
+                   "incremental_ms": runs[True][0], "updated_sweeps": runs[True][1]}
+
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu:
@@ -295,6 +316,7 @@ def run_engine(args, g, world, rank, local, pg):
                          "kernel": "k_profit", "kernel_ms": prof_ms, "alg_bytes": alg_bytes,
                          "min_terms": terms},
             "sweep_roofline_int32": sweep_roof,
+            "descent": descent,
             "cpu_baseline": cpu,
             "gpu_launches": args.steps * (OWN_KERNELS_PER_SWEEP + CUB_KERNELS_PER_SWEEP),
             "clocks": clk.summary(),
@@ -581,6 +603,7 @@ def main():
     ap.add_argument("--pre-sweeps", type=int, default=50)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-descent", action="store_true", help="skip the time-to-convergence descents")
     args = ap.parse_args()
     world, rank, local, pg = dist_setup()
     import bm

@@ -65,6 +65,10 @@ class LookupStats(C.Structure):
                 ("ms_refresh", C.c_float), ("ms_total", C.c_float)]
 
 
+class GreedyStats(C.Structure):
+    _fields_ = [("ms_features", C.c_float), ("ms_match", C.c_float), ("reserved", C.c_int32 * 2)]
+
+
 class MlpTrainStats(C.Structure):
     _fields_ = [("samples", C.c_int64), ("steps", C.c_int64), ("first_loss", C.c_float), ("last_loss", C.c_float)]
 
@@ -128,6 +132,8 @@ def lib():
         L.bm_triple_round.argtypes = [vp, C.POINTER(TripleOpts), C.POINTER(TripleStats)]
         L.bm_lookup_rows.argtypes = [vp, i32, i32, vp]
         L.bm_lookup_descent.argtypes = [vp, i32, C.POINTER(LookupStats)]
+        L.bm_greedy_match.argtypes = [i32, i64, vp, vp, vp, i64, vp, vp, vp, vp, C.POINTER(GreedyStats)]
+        L.bm_greedy_features.argtypes = [i32, i64, vp, vp, vp, vp]
         L.bm_timer_mark.argtypes = [vp, i32]
         L.bm_timer_elapsed.argtypes = [vp, i32, i32, C.POINTER(C.c_float)]
         L.bm_measure_peaks.argtypes = [i32, C.POINTER(C.c_double), C.POINTER(C.c_double)]
@@ -376,6 +382,25 @@ def write_mapping_csv(path, m, numeric=False):
     m = np.ascontiguousarray(m, np.int32)
     f = lib().bm_write_mapping_csv_numeric if numeric else lib().bm_write_mapping_csv
     _check(f(path.encode(), len(m) - 1, _p(m)))
+
+
+def greedy_match(g):
+    """Greedy feature matcher (bm_greedy_match): (map int32[n+1], stats dict)."""
+    n = int(g["n"])
+    a = [np.ascontiguousarray(g[k], np.int32) for k in ("src1", "dst1", "w1", "src2", "dst2", "w2")]
+    m = np.zeros(n + 1, np.int32)
+    st = GreedyStats()
+    _check(lib().bm_greedy_match(n, len(a[0]), _p(a[0]), _p(a[1]), _p(a[2]), len(a[3]), _p(a[3]), _p(a[4]),
+                                 _p(a[5]), _p(m), C.byref(st)))
+    return m, {"ms_features": st.ms_features, "ms_match": st.ms_match}
+
+
+def greedy_features(n, src, dst, w):
+    """[n, 4] int32: in-degree, out-degree, distinct 2-hop out-reach, 2-hop in-reach."""
+    s, d, ww = (np.ascontiguousarray(x, np.int32) for x in (src, dst, w))
+    out = np.zeros((int(n), 4), np.int32)
+    _check(lib().bm_greedy_features(int(n), len(s), _p(s), _p(d), _p(ww), _p(out)))
+    return out
 
 
 def measure_peaks(n):

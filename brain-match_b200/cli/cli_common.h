@@ -3,7 +3,9 @@
  *
  * Each tool keeps the reference tool's argv and file formats; the search
  * itself runs on the GPU through the C ABI (include/bm.h).  Knobs that the
- * reference hard-codes are read from BM_* environment variables.
+ * reference hard-codes are read from BM_* environment variables (BM_INCREMENTAL=0
+ * rebuilds the profit matrix every sweep instead of updating it; the results
+ * are the same).
  */
 #ifndef BM_CLI_COMMON_H
 #define BM_CLI_COMMON_H
@@ -95,6 +97,7 @@ static inline long long cli_sweeps(cli_job* j, int max_sweeps, int verbose) {
     memset(&o, 0, sizeof o);
     o.max_candidates = (int)env_long("BM_MAX_CANDIDATES", 0);
     o.max_verify = (int)env_long("BM_MAX_VERIFY", -1);
+    o.incremental = (int)env_long("BM_INCREMENTAL", 1);
     long long commits = 0;
     for (int s = 0; s < max_sweeps; s++) {
         bm_sweep_stats st;

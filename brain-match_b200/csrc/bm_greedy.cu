@@ -1,0 +1,482 @@
+// bm_greedy.cu -- the greedy feature matcher (src/greedy-feature-match.c:
+// 527-712) on the GPU: an initial matching for the swap search.
+//
+// Vertex features (compute_vertex_features, :527-566): in- and out-degree
+// (every list entry: repeated edges and self-loops count), the number of
+// distinct vertices reachable in exactly two out-steps and the number that
+// reach the vertex in two in-steps, and their sum ("total").  G1 vertices are
+// matched one at a time in order of total (descending; ties by id, where the
+// reference's qsort leaves the order unspecified), each to the unmatched G2
+// vertex of largest
+//     0.3 * -distance + 0.7 * align            (:633-647)
+// with distance = (int)(1000 * sum_k |ratio1_k - ratio2_k|) over the four
+// feature/total ratios (compute_feature_distance, :575-586) and align the
+// edge overlap with the G1 neighbours matched so far:
+//     sum_{v1->t, t matched} min(w, W2[v2][m t]) + sum_{s->v1, s matched} min(w, W2[m s][v2])
+// (compute_edge_alignment, :297-356, with its evident intent: the reference
+// compares G2 ids against G2 indices and tests a G1 vertex against G2 position
+// flags).  Among equal scores the first candidate in G2's feature order wins,
+// as the reference's strict ">" does.  A vertex without any edge (total 0,
+// where the reference divides 0/0) has all ratios 0.  W2 is the last weight
+// given for a G2 pair, which is what the reference's prepended lists find first.
+//
+// The sequential loop runs as one cooperative grid, a CTA per SM: each step
+// scatters the align terms through the G2 lists of the matched neighbours'
+// images into an L2-resident array (the edges spread over the CTAs), every
+// CTA takes the best of its own slice of candidates, and every CTA reduces
+// the published slice bests -- two bounded grid barriers per step.
+#include <cub/cub.cuh>
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "bm.h"
+#include "bm_internal.cuh"
+
+namespace bm {
+namespace {
+
+constexpr int kGreedyThreads = 512;
+constexpr unsigned kGreedySpinLimit = 1u << 24;  // polls of one grid-barrier wait (~1 s)
+
+struct GreedyBest {
+    double score;
+    int pos;  // candidate's place in G2's feature order
+    int g;    // candidate (0-based), -1 none
+};
+
+__device__ __forceinline__ bool better(const GreedyBest& x, const GreedyBest& y) {
+    return x.score > y.score || (x.score == y.score && x.pos < y.pos);
+}
+
+// Distinct vertices at the end of a two-step walk along the lists (off, id):
+// cnt[u] = |{w : u -> v -> w}|.  One CTA per vertex, a bitmap of n bits in
+// shared memory.
+__global__ void k_two_hop(const int* __restrict__ off, const int* __restrict__ id, int n, int* __restrict__ cnt) {
+    extern __shared__ unsigned bits[];
+    __shared__ int part[32];
+    const int words = (n + 31) >> 5;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int u = blockIdx.x; u < n; u += gridDim.x) {
+        for (int i = threadIdx.x; i < words; i += blockDim.x) bits[i] = 0u;
+        __syncthreads();
+        for (int j = off[u] + wid; j < off[u + 1]; j += nw) {
+            const int v = id[j];
+            for (int k = off[v] + lane; k < off[v + 1]; k += 32) {
+                const int w = id[k];
+                atomicOr(&bits[w >> 5], 1u << (w & 31));
+            }
+        }
+        __syncthreads();
+        int c = 0;
+        for (int i = threadIdx.x; i < words; i += blockDim.x) c += __popc(bits[i]);
+        for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        if (lane == 0) part[wid] = c;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int t = 0;
+            for (int w = 0; w < nw; w++) t += part[w];
+            cnt[u] = t;
+        }
+        __syncthreads();
+    }
+}
+
+// Features (in, out, 2-hop out, 2-hop in), the four ratios to their total and
+// the sort key (total descending, id ascending).
+__global__ void k_features(const int* __restrict__ offo, const int* __restrict__ offi, const int* __restrict__ r2,
+                           const int* __restrict__ c2, int n, int4* __restrict__ feat, double4* __restrict__ ratio,
+                           unsigned long long* __restrict__ key, int* __restrict__ val) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    const int in = offi[v + 1] - offi[v], out = offo[v + 1] - offo[v];
+    const int4 f = make_int4(in, out, r2[v], c2[v]);
+    const int total = f.x + f.y + f.z + f.w;
+    feat[v] = f;
+    double4 r = make_double4(0.0, 0.0, 0.0, 0.0);
+    if (total > 0) {
+        const double t = (double)total;
+        r = make_double4(__ddiv_rn((double)f.x, t), __ddiv_rn((double)f.y, t), __ddiv_rn((double)f.z, t),
+                         __ddiv_rn((double)f.w, t));
+    }
+    ratio[v] = r;
+    key[v] = ((unsigned long long)(0xffffffffu - (unsigned)total) << 32) | (unsigned)v;
+    val[v] = v;
+}
+
+__global__ void k_positions(const int* __restrict__ order, int n, int* __restrict__ pos) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) pos[order[i]] = i;
+}
+
+struct GreedyArgs {
+    int n, slice;
+    const int *off1o, *id1o, *w1o, *off1i, *id1i, *w1i;  // G1, every entry
+    const int *off2o, *id2o, *w2o, *off2i, *id2i, *w2i;  // G2, one entry per pair (last weight)
+    const int* order1;                                    // G1 in feature order
+    const int* pos2;                                      // G2 vertex -> place in feature order
+    const double4 *ratio1, *ratio2;
+    int* acc;                                             // n align sums, zero between steps
+    GreedyBest* bests;                                    // [2][gridDim.x] per-CTA bests
+    unsigned* bar;                                        // [0] arrivals [1] generation [2] error
+    int* map;                                             // out: G1 -> G2 (0-based)
+};
+
+// Score of candidate g for the G1 vertex with ratios r1: the reference's
+// double arithmetic, every operation rounded once (no contraction).
+__device__ __forceinline__ double greedy_score(const double4& r1, const double4& r2, int align) {
+    double d = fabs(__dsub_rn(r1.x, r2.x));
+    d = __dadd_rn(d, fabs(__dsub_rn(r1.y, r2.y)));
+    d = __dadd_rn(d, fabs(__dsub_rn(r1.z, r2.z)));
+    d = __dadd_rn(d, fabs(__dsub_rn(r1.w, r2.w)));
+    const int dist = __double2int_rz(__dmul_rn(d, 1000.0));
+    return __dadd_rn(__dmul_rn(0.3, (double)(-dist)), __dmul_rn(0.7, (double)align));
+}
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Grid-wide barrier of the co-resident CTAs.  Each wait is bounded: after
+// kGreedySpinLimit polls the CTA records the error word and every CTA leaves
+// at its next barrier.  Returns false once the error word is set.
+__device__ bool grid_barrier(unsigned* bar) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        __threadfence();
+        const unsigned gen = ld_acquire_u32(&bar[1]);
+        if (atomicAdd(&bar[0], 1u) == gridDim.x - 1) {
+            atomicExch(&bar[0], 0u);
+            __threadfence();
+            atomicAdd(&bar[1], 1u);
+        } else {
+            unsigned it = 0;
+            while (ld_acquire_u32(&bar[1]) == gen) {
+                if (ld_acquire_u32(&bar[2]) || ++it > kGreedySpinLimit) {
+                    atomicExch(&bar[2], 1u);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        s_ok = ok && !ld_acquire_u32(&bar[2]);
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// The sequential matching, one CTA per SM (cooperative launch).  Step i:
+// every warp scatters the align terms of one of v1's edges into acc (global,
+// L2-resident), then every CTA takes the best candidate of its own slice of G2, then
+// all CTAs reduce the slices' bests, each from the same published array.
+__global__ void __launch_bounds__(kGreedyThreads, 1) k_greedy(GreedyArgs a) {
+    extern __shared__ int gsm[];
+    int* map_s = gsm;                                   // n: G1 -> G2, -1 unmatched (a copy per CTA)
+    int* pos_s = map_s + a.n;                           // slice
+    unsigned char* taken = reinterpret_cast<unsigned char*>(pos_s + a.slice);
+    __shared__ GreedyBest wbest[kGreedyThreads / 32];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int base = blockIdx.x * a.slice;
+    const int len = max(0, min(a.slice, a.n - base));
+    for (int i = tid; i < a.n; i += blockDim.x) map_s[i] = -1;
+    for (int l = tid; l < a.slice; l += blockDim.x) {
+        taken[l] = l < len ? 0 : 1;
+        pos_s[l] = l < len ? a.pos2[base + l] : 0x7fffffff;
+    }
+    __syncthreads();
+    const int gw = blockIdx.x * (kGreedyThreads / 32) + wid, nwarps = gridDim.x * (kGreedyThreads / 32);
+    for (int step = 0; step < a.n; step++) {
+        const int par = step & 1;
+        const int v1 = a.order1[step];
+        // ---- align terms: edge j of v1 to warp j of the grid, its G2 list over the lanes ----
+        const int o0 = a.off1o[v1], dout = a.off1o[v1 + 1] - o0;
+        const int i0 = a.off1i[v1], din = a.off1i[v1 + 1] - i0;
+        for (int j = gw; j < dout + din; j += nwarps) {
+            const bool out = j < dout;
+            const int t = out ? a.id1o[o0 + j] : a.id1i[i0 + j - dout];
+            const int w = out ? a.w1o[o0 + j] : a.w1i[i0 + j - dout];
+            const int f = map_s[t];
+            if (f < 0 || w <= 0) continue;
+            const int* off = out ? a.off2i : a.off2o;
+            const int* lid = out ? a.id2i : a.id2o;
+            const int* lw = out ? a.w2i : a.w2o;
+            for (int k = off[f] + lane; k < off[f + 1]; k += 32) {
+                const int c = min(w, lw[k]);
+                if (c > 0) atomicAdd(&a.acc[lid[k]], c);
+            }
+        }
+        if (!grid_barrier(a.bar)) return;
+        // ---- this CTA's best candidate (and acc cleared for the next step) ----
+        const double4 r1 = a.ratio1[v1];
+        GreedyBest best{-1.0 / 0.0, 0x7fffffff, -1};
+        for (int l = tid; l < len; l += blockDim.x) {
+            const int al = __ldcg(&a.acc[base + l]);
+            if (al) a.acc[base + l] = 0;
+            if (taken[l]) continue;
+            const GreedyBest c{greedy_score(r1, a.ratio2[base + l], al), pos_s[l], base + l};
+            if (better(c, best)) best = c;
+        }
+        for (int o = 16; o; o >>= 1) {
+            GreedyBest y;
+            y.score = __shfl_xor_sync(0xffffffffu, best.score, o);
+            y.pos = __shfl_xor_sync(0xffffffffu, best.pos, o);
+            y.g = __shfl_xor_sync(0xffffffffu, best.g, o);
+            if (better(y, best)) best = y;
+        }
+        if (lane == 0) wbest[wid] = best;
+        __syncthreads();
+        if (tid == 0) {
+            for (int w = 1; w < kGreedyThreads / 32; w++)
+                if (better(wbest[w], best)) best = wbest[w];
+            GreedyBest* dst = a.bests + par * gridDim.x + blockIdx.x;
+            __stcg(&dst->score, best.score);
+            __stcg(&dst->pos, best.pos);
+            __stcg(&dst->g, best.g);
+        }
+        if (!grid_barrier(a.bar)) return;
+        // ---- the grid's best, reduced by every CTA from the published bests ----
+        best = GreedyBest{-1.0 / 0.0, 0x7fffffff, -1};
+        for (int r = tid; r < (int)gridDim.x; r += blockDim.x) {
+            const GreedyBest* src = a.bests + par * gridDim.x + r;
+            const GreedyBest c{__ldcg(&src->score), __ldcg(&src->pos), __ldcg(&src->g)};
+            if (better(c, best)) best = c;
+        }
+        for (int o = 16; o; o >>= 1) {
+            GreedyBest y;
+            y.score = __shfl_xor_sync(0xffffffffu, best.score, o);
+            y.pos = __shfl_xor_sync(0xffffffffu, best.pos, o);
+            y.g = __shfl_xor_sync(0xffffffffu, best.g, o);
+            if (better(y, best)) best = y;
+        }
+        if (lane == 0) wbest[wid] = best;
+        __syncthreads();
+        if (tid == 0) {
+            for (int w = 1; w < kGreedyThreads / 32; w++)
+                if (better(wbest[w], best)) best = wbest[w];
+            map_s[v1] = best.g;
+            if (best.g >= base && best.g < base + len) taken[best.g - base] = 1;
+            if (blockIdx.x == 0) a.map[v1] = best.g;
+        }
+        __syncthreads();
+    }
+}
+
+struct HostLists {
+    std::vector<int> off, id, w;
+};
+
+// CSR keyed by key[] (every entry, input order within a row).
+void host_csr(int n, long long m, const int* key, const int* other, const int* w, HostLists& L) {
+    L.off.assign((size_t)n + 1, 0);
+    for (long long i = 0; i < m; i++) L.off[key[i] + 1]++;
+    for (int v = 0; v < n; v++) L.off[v + 1] += L.off[v];
+    std::vector<int> pos(L.off.begin(), L.off.end() - 1);
+    L.id.resize(m);
+    L.w.resize(m);
+    for (long long i = 0; i < m; i++) {
+        const int p = pos[key[i]]++;
+        L.id[p] = other[i];
+        L.w[p] = w[i];
+    }
+}
+
+struct GreedyDev {
+    std::vector<void*> bufs;
+    ~GreedyDev() { for (void* p : bufs) cudaFree(p); }
+    template <class T> cudaError_t alloc(T** p, size_t count) {
+        cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(count, 1) * sizeof(T));
+        if (e == cudaSuccess) bufs.push_back(*p);
+        return e;
+    }
+    template <class T> cudaError_t up(T** p, const std::vector<T>& h) {
+        cudaError_t e = alloc(p, h.size());
+        if (e == cudaSuccess && !h.empty()) e = cudaMemcpy(*p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
+        return e;
+    }
+};
+
+#define GK(call)                                                                      \
+    do {                                                                              \
+        cudaError_t _e = (call);                                                      \
+        if (_e != cudaSuccess) {                                                      \
+            set_err(nullptr, "%s: %s (%s:%d)", fn, cudaGetErrorString(_e), __FILE__, __LINE__); \
+            return BM_E_CUDA;                                                         \
+        }                                                                             \
+    } while (0)
+
+// Validates one graph's edges and converts ids to 0-based.
+bm_status load_edges(const char* fn, int n, long long m, const int32_t* s, const int32_t* d, const int32_t* w,
+                     std::vector<int>& s0, std::vector<int>& d0, std::vector<int>& w0) {
+    if (m < 0 || (m > 0 && (!s || !d || !w))) { set_err(nullptr, "%s: bad edge arrays", fn); return BM_E_INPUT; }
+    s0.resize(m); d0.resize(m); w0.resize(m);
+    for (long long i = 0; i < m; i++) {
+        if (s[i] < 1 || s[i] > n || d[i] < 1 || d[i] > n) {
+            set_err(nullptr, "%s: edge %lld (%d,%d) outside 1..%d", fn, i, s[i], d[i], n);
+            return BM_E_INPUT;
+        }
+        if (w[i] < 0) { set_err(nullptr, "%s: edge %lld has negative weight %d", fn, i, w[i]); return BM_E_INPUT; }
+        s0[i] = s[i] - 1; d0[i] = d[i] - 1; w0[i] = w[i];
+    }
+    return BM_OK;
+}
+
+// Features of one graph on the device: feat (int4), ratio (double4), and the
+// feature order (order[i] = vertex at place i).
+bm_status device_features(const char* fn, GreedyDev& D, int n, const HostLists& lo, const HostLists& li,
+                          int4* feat, double4* ratio, int* order, cudaStream_t st, int sms) {
+    int *offo, *ido, *offi, *idi, *r2, *c2, *val, *val2;
+    unsigned long long *key, *key2;
+    GK(D.up(&offo, lo.off)); GK(D.up(&ido, lo.id));
+    GK(D.up(&offi, li.off)); GK(D.up(&idi, li.id));
+    GK(D.alloc(&r2, n)); GK(D.alloc(&c2, n));
+    GK(D.alloc(&key, n)); GK(D.alloc(&key2, n)); GK(D.alloc(&val, n)); GK(D.alloc(&val2, n));
+    const size_t bm = (size_t)((n + 31) / 32) * sizeof(unsigned);
+    GK(cudaFuncSetAttribute(k_two_hop, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bm));
+    k_two_hop<<<sms * 4, 512, bm, st>>>(offo, ido, n, r2);
+    k_two_hop<<<sms * 4, 512, bm, st>>>(offi, idi, n, c2);
+    k_features<<<(n + 255) / 256, 256, 0, st>>>(offo, offi, r2, c2, n, feat, ratio, key, val);
+    GK(cudaGetLastError());
+    size_t tb = 0;
+    GK(cub::DeviceRadixSort::SortPairs(nullptr, tb, key, key2, val, val2, n, 0, 64, st));
+    void* tmp;
+    GK(D.alloc((char**)&tmp, tb));
+    GK(cub::DeviceRadixSort::SortPairs(tmp, tb, key, key2, val, order, n, 0, 64, st));
+    return BM_OK;
+}
+
+}  // namespace
+}  // namespace bm
+
+using namespace bm;
+
+extern "C" bm_status bm_greedy_features(int32_t n, int64_t e, const int32_t* src, const int32_t* dst,
+                                        const int32_t* w, int32_t* out) {
+    const char* fn = "bm_greedy_features";
+    if (n < 1 || !out) { set_err(nullptr, "%s: bad arguments", fn); return BM_E_INPUT; }
+    std::vector<int> s0, d0, w0;
+    bm_status s = load_edges(fn, n, e, src, dst, w, s0, d0, w0);
+    if (s) return s;
+    HostLists lo, li;
+    host_csr(n, e, s0.data(), d0.data(), w0.data(), lo);
+    host_csr(n, e, d0.data(), s0.data(), w0.data(), li);
+    int dev = 0, sms = 0;
+    GK(cudaGetDevice(&dev));
+    GK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    GreedyDev D;
+    int4* feat; double4* ratio; int* order;
+    GK(D.alloc(&feat, n)); GK(D.alloc(&ratio, n)); GK(D.alloc(&order, n));
+    s = device_features(fn, D, n, lo, li, feat, ratio, order, 0, sms);
+    if (s) return s;
+    GK(cudaMemcpy(out, feat, (size_t)n * sizeof(int4), cudaMemcpyDeviceToHost));
+    return BM_OK;
+}
+
+extern "C" bm_status bm_greedy_match(int32_t n, int64_t e1, const int32_t* src1, const int32_t* dst1,
+                                     const int32_t* w1, int64_t e2, const int32_t* src2, const int32_t* dst2,
+                                     const int32_t* w2, int32_t* map, bm_greedy_stats* stats) {
+    const char* fn = "bm_greedy_match";
+    if (n < 1 || !map) { set_err(nullptr, "%s: bad arguments", fn); return BM_E_INPUT; }
+    std::vector<int> s1, d1, ww1, s2, d2, ww2;
+    bm_status s = load_edges(fn, n, e1, src1, dst1, w1, s1, d1, ww1);
+    if (!s) s = load_edges(fn, n, e2, src2, dst2, w2, s2, d2, ww2);
+    if (s) return s;
+    HostLists g1o, g1i, g2o, g2i, g2od, g2id;
+    host_csr(n, e1, s1.data(), d1.data(), ww1.data(), g1o);
+    host_csr(n, e1, d1.data(), s1.data(), ww1.data(), g1i);
+    host_csr(n, e2, s2.data(), d2.data(), ww2.data(), g2o);
+    host_csr(n, e2, d2.data(), s2.data(), ww2.data(), g2i);
+    {   // G2 with one entry per (src, dst): the last weight given
+        std::vector<int> keep;
+        keep.reserve(e2);
+        std::vector<int> last((size_t)n, -1);
+        for (int u = 0; u < n; u++) {
+            // the last occurrence of each dst in u's row (rows keep input order)
+            for (int k = g2o.off[u + 1] - 1; k >= g2o.off[u]; k--) {
+                const int v = g2o.id[k];
+                if (last[v] == u) continue;
+                last[v] = u;
+                keep.push_back(k);
+            }
+        }
+        std::vector<int> ks(keep.size()), kd(keep.size()), kw(keep.size());
+        std::vector<int> rowof(e2);
+        for (int u = 0; u < n; u++)
+            for (int k = g2o.off[u]; k < g2o.off[u + 1]; k++) rowof[k] = u;
+        for (size_t i = 0; i < keep.size(); i++) {
+            ks[i] = rowof[keep[i]]; kd[i] = g2o.id[keep[i]]; kw[i] = g2o.w[keep[i]];
+        }
+        host_csr(n, (long long)keep.size(), ks.data(), kd.data(), kw.data(), g2od);
+        host_csr(n, (long long)keep.size(), kd.data(), ks.data(), kw.data(), g2id);
+    }
+    int dev = 0, sms = 0, optin = 0;
+    GK(cudaGetDevice(&dev));
+    GK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    GK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    int per_sm = 0;
+    const int slice0 = (n + sms - 1) / sms;
+    size_t smem = (size_t)n * 4 + (size_t)slice0 * 5 + 16;
+    if (smem + 4096 > (size_t)optin) {
+        set_err(nullptr, "%s: n=%d needs %zu bytes of shared memory per CTA (limit %d)", fn, n, smem, optin);
+        return BM_E_INPUT;
+    }
+    GK(cudaFuncSetAttribute(k_greedy, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    GK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_greedy, kGreedyThreads, smem));
+    if (per_sm < 1) { set_err(nullptr, "%s: the matching kernel does not fit on an SM", fn); return BM_E_INPUT; }
+    const int grid = sms;
+    cudaStream_t st;
+    GK(cudaStreamCreate(&st));
+    struct StreamGuard { cudaStream_t s; ~StreamGuard() { cudaStreamSynchronize(s); cudaStreamDestroy(s); } } sg{st};
+    cudaEvent_t ev[3];
+    for (auto& e : ev) GK(cudaEventCreate(&e));
+    struct EvGuard { cudaEvent_t* e; ~EvGuard() { for (int i = 0; i < 3; i++) cudaEventDestroy(e[i]); } } eg{ev};
+    GreedyDev D;
+    int4 *feat1, *feat2;
+    double4 *ratio1, *ratio2;
+    int *order1, *order2, *pos2, *mapd, *acc;
+    GreedyBest* bests;
+    unsigned* bar;
+    GK(D.alloc(&feat1, n)); GK(D.alloc(&feat2, n)); GK(D.alloc(&ratio1, n)); GK(D.alloc(&ratio2, n));
+    GK(D.alloc(&order1, n)); GK(D.alloc(&order2, n)); GK(D.alloc(&pos2, n)); GK(D.alloc(&mapd, n));
+    GK(D.alloc(&acc, n)); GK(D.alloc(&bests, 2 * (size_t)grid)); GK(D.alloc(&bar, 4));
+    GK(cudaMemsetAsync(acc, 0, (size_t)n * sizeof(int), st));
+    GK(cudaMemsetAsync(bar, 0, 4 * sizeof(unsigned), st));
+    GreedyArgs A;
+    A.n = n; A.slice = slice0;
+    int* p;
+    GK(D.up(&p, g1o.off)); A.off1o = p; GK(D.up(&p, g1o.id)); A.id1o = p; GK(D.up(&p, g1o.w)); A.w1o = p;
+    GK(D.up(&p, g1i.off)); A.off1i = p; GK(D.up(&p, g1i.id)); A.id1i = p; GK(D.up(&p, g1i.w)); A.w1i = p;
+    GK(D.up(&p, g2od.off)); A.off2o = p; GK(D.up(&p, g2od.id)); A.id2o = p; GK(D.up(&p, g2od.w)); A.w2o = p;
+    GK(D.up(&p, g2id.off)); A.off2i = p; GK(D.up(&p, g2id.id)); A.id2i = p; GK(D.up(&p, g2id.w)); A.w2i = p;
+    GK(cudaEventRecord(ev[0], st));
+    s = device_features(fn, D, n, g1o, g1i, feat1, ratio1, order1, st, sms);
+    if (!s) s = device_features(fn, D, n, g2o, g2i, feat2, ratio2, order2, st, sms);
+    if (s) return s;
+    k_positions<<<(n + 255) / 256, 256, 0, st>>>(order2, n, pos2);
+    GK(cudaGetLastError());
+    GK(cudaEventRecord(ev[1], st));
+    A.order1 = order1; A.pos2 = pos2; A.ratio1 = ratio1; A.ratio2 = ratio2;
+    A.acc = acc; A.bests = bests; A.bar = bar; A.map = mapd;
+    void* kargs[] = {&A};
+    GK(cudaLaunchCooperativeKernel((const void*)k_greedy, dim3(grid), dim3(kGreedyThreads), kargs, smem, st));
+    GK(cudaEventRecord(ev[2], st));
+    unsigned herr[4] = {0, 0, 0, 0};
+    GK(cudaMemcpyAsync(herr, bar, sizeof herr, cudaMemcpyDeviceToHost, st));
+    std::vector<int> h(n);
+    GK(cudaMemcpyAsync(h.data(), mapd, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, st));
+    GK(cudaStreamSynchronize(st));
+    if (herr[2]) { set_err(nullptr, "%s: grid barrier wait timed out", fn); return BM_E_TIMEOUT; }
+    map[0] = 0;
+    for (int v = 0; v < n; v++) map[v + 1] = h[v] + 1;
+    if (stats) {
+        memset(stats, 0, sizeof *stats);
+        cudaEventElapsedTime(&stats->ms_features, ev[0], ev[1]);
+        cudaEventElapsedTime(&stats->ms_match, ev[1], ev[2]);
+    }
+    return BM_OK;
+}

@@ -545,6 +545,37 @@ bm_status bm_learned_run(bm_ctx* ctx, bm_mlp* m, const bm_learned_opts* opts, in
                          int64_t target_score, int32_t probe_every, bm_learned_run_stats* stats,
                          int64_t* trace_score, float* trace_ms, int8_t* trace_kind);
 
+/* ---- Initial matching: the greedy feature matcher ----
+ * src/greedy-feature-match.c:527-712.  G1 vertices, in order of their
+ * feature total (in-degree + out-degree + distinct 2-hop out-reach + distinct
+ * 2-hop in-reach; descending, ties by id), each take the unmatched G2 vertex of
+ * largest 0.3 * -distance + 0.7 * align: distance = (int)(1000 * sum |r1 - r2|)
+ * over the four feature / total ratios, align = sum of min(w1, w2) over the
+ * vertex's G1 edges to already matched neighbours and the corresponding G2
+ * edges of the candidate; equal scores go to the candidate first in G2's
+ * feature order.  Degrees count every edge given (repeats and self-loops); W2
+ * is the last weight given for a G2 pair.  A vertex without edges has ratios 0
+ * (the reference divides 0/0 there), and align compares G2 vertices with G2
+ * vertices (the reference compares ids with indices).  Independent of any
+ * bm_ctx; runs on the current device. */
+typedef struct {
+    float ms_features;   /* device time of both graphs' features and orders */
+    float ms_match;      /* device time of the sequential matching          */
+    int32_t reserved[2];
+} bm_greedy_stats;
+
+/* map (n+1 entries) receives the matching, 1-based, map[0] = 0.  Errors are
+ * reported by bm_last_error(NULL). */
+bm_status bm_greedy_match(int32_t n, int64_t e1, const int32_t* src1, const int32_t* dst1, const int32_t* w1,
+                          int64_t e2, const int32_t* src2, const int32_t* dst2, const int32_t* w2,
+                          int32_t* map, bm_greedy_stats* stats);
+
+/* The features of one graph (compute_vertex_features, :527-566):
+ * out[4(v-1) + k] for v = 1..n, k = in-degree, out-degree, distinct 2-hop
+ * out-reach, distinct 2-hop in-reach. */
+bm_status bm_greedy_features(int32_t n, int64_t e, const int32_t* src, const int32_t* dst, const int32_t* w,
+                             int32_t* out);
+
 /* ---- Host utilities: file formats and the synthetic generator ---- */
 
 /* Free memory returned by the readers below. */

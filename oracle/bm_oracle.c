@@ -17,6 +17,11 @@
  *   orc_best_swap_descent  the extract_max / swap / update loop of the
  *                      best-swap tool (src/best-swap/score-lookup.c:597-640)
  *                      on an exact delta table, largest delta first
+ *   orc_greedy_features / orc_greedy_distance / orc_greedy_match  the
+ *                      greedy feature matcher (src/greedy-feature-match.c:
+ *                      527-712): compute_vertex_features,
+ *                      compute_feature_distance and match_vertices with
+ *                      compute_edge_alignment's evident intent
  *   orc_sweep / orc_triple_round / orc_quad_round  the best-per-row set commit that the engine
  *                      runs (candidates sorted by delta desc then ids, each
  *                      re-verified on the updated mapping).
@@ -32,6 +37,7 @@
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
+#include <math.h>
 
 #define MIN(a, b) ((a) < (b) ? (a) : (b))
 
@@ -575,4 +581,179 @@ int orc_best_swap_descent(void* p, int* map, int max_swaps, int* swaps, int* del
         done++;
     }
     return done;
+}
+
+/* ---- greedy feature matcher (src/greedy-feature-match.c:527-712) ---- */
+
+typedef struct { int *off, *id, *w; } glists;
+
+/* rows keyed by key[] (0-based), every entry, input order within a row */
+static void g_csr(int n, long long m, const int* key, const int* other, const int* w, glists* L) {
+    L->off = (int*)calloc((size_t)n + 1, sizeof(int));
+    L->id = (int*)malloc(sizeof(int) * (size_t)(m ? m : 1));
+    L->w = (int*)malloc(sizeof(int) * (size_t)(m ? m : 1));
+    for (long long i = 0; i < m; i++) L->off[key[i] + 1]++;
+    for (int v = 0; v < n; v++) L->off[v + 1] += L->off[v];
+    int* pos = (int*)malloc(sizeof(int) * (size_t)(n ? n : 1));
+    memcpy(pos, L->off, sizeof(int) * (size_t)n);
+    for (long long i = 0; i < m; i++) {
+        const int p = pos[key[i]]++;
+        L->id[p] = other[i];
+        L->w[p] = w ? w[i] : 0;
+    }
+    free(pos);
+}
+
+static void g_free(glists* L) { free(L->off); free(L->id); free(L->w); }
+
+/* distinct w with u -> v -> w along L */
+static int g_two_hop(const glists* L, int n, int u, unsigned char* seen) {
+    int c = 0;
+    memset(seen, 0, (size_t)n);
+    for (int j = L->off[u]; j < L->off[u + 1]; j++) {
+        const int v = L->id[j];
+        for (int k = L->off[v]; k < L->off[v + 1]; k++)
+            if (!seen[L->id[k]]) { seen[L->id[k]] = 1; c++; }
+    }
+    return c;
+}
+
+/* compute_vertex_features (:527-566) over 1-based edges: feat[4(v-1)+k] =
+ * in-degree, out-degree, 2-hop reachable, 2-hop can-reach (every edge entry
+ * counts, self-loops and repeats included). */
+void orc_greedy_features(int n, long long e, const int* src, const int* dst, int* feat) {
+    int* s0 = (int*)malloc(sizeof(int) * (size_t)(e ? e : 1));
+    int* d0 = (int*)malloc(sizeof(int) * (size_t)(e ? e : 1));
+    for (long long i = 0; i < e; i++) { s0[i] = src[i] - 1; d0[i] = dst[i] - 1; }
+    glists lo, li;
+    g_csr(n, e, s0, d0, NULL, &lo);
+    g_csr(n, e, d0, s0, NULL, &li);
+    #pragma omp parallel
+    {
+        unsigned char* seen = (unsigned char*)malloc((size_t)n + 1);
+        #pragma omp for schedule(dynamic, 16)
+        for (int v = 0; v < n; v++) {
+            feat[4 * v + 0] = li.off[v + 1] - li.off[v];
+            feat[4 * v + 1] = lo.off[v + 1] - lo.off[v];
+            feat[4 * v + 2] = g_two_hop(&lo, n, v, seen);
+            feat[4 * v + 3] = g_two_hop(&li, n, v, seen);
+        }
+        free(seen);
+    }
+    g_free(&lo); g_free(&li); free(s0); free(d0);
+}
+
+static void g_ratios(const int* f, double* r) {
+    const int total = f[0] + f[1] + f[2] + f[3];
+    for (int k = 0; k < 4; k++) r[k] = total > 0 ? (double)f[k] / (double)total : 0.0;
+}
+
+static int g_distance(const double* r1, const double* r2) {
+    const double d1 = fabs(r1[0] - r2[0]), d2 = fabs(r1[1] - r2[1]);
+    const double d3 = fabs(r1[2] - r2[2]), d4 = fabs(r1[3] - r2[3]);
+    return (int)((d1 + d2 + d3 + d4) * 1000);
+}
+
+/* compute_feature_distance (:575-586) of two feature rows (in, out, r2, c2);
+ * a row whose total is 0 has ratios 0. */
+int orc_greedy_distance(const int* f1, const int* f2) {
+    double r1[4], r2[4];
+    g_ratios(f1, r1);
+    g_ratios(f2, r2);
+    return g_distance(r1, r2);
+}
+
+typedef struct { unsigned total; int v; } g_key;
+static int g_cmp(const void* a, const void* b) {
+    const g_key* x = (const g_key*)a;
+    const g_key* y = (const g_key*)b;
+    if (x->total != y->total) return x->total > y->total ? -1 : 1;
+    return x->v < y->v ? -1 : (x->v > y->v);
+}
+
+/* match_vertices (:588-676): map[v] (1-based, n+1 entries) = the G2 vertex
+ * chosen for G1 vertex v. */
+void orc_greedy_match(int n, long long e1, const int* s1, const int* d1, const int* w1,
+                      long long e2, const int* s2, const int* d2, const int* w2, int* map) {
+    int* f1 = (int*)malloc(sizeof(int) * 4 * (size_t)n);
+    int* f2 = (int*)malloc(sizeof(int) * 4 * (size_t)n);
+    orc_greedy_features(n, e1, s1, d1, f1);
+    orc_greedy_features(n, e2, s2, d2, f2);
+    double* r1 = (double*)malloc(sizeof(double) * 4 * (size_t)n);
+    double* r2 = (double*)malloc(sizeof(double) * 4 * (size_t)n);
+    g_key* k1 = (g_key*)malloc(sizeof(g_key) * (size_t)n);
+    g_key* k2 = (g_key*)malloc(sizeof(g_key) * (size_t)n);
+    for (int v = 0; v < n; v++) {
+        g_ratios(f1 + 4 * v, r1 + 4 * v);
+        g_ratios(f2 + 4 * v, r2 + 4 * v);
+        k1[v].total = (unsigned)(f1[4 * v] + f1[4 * v + 1] + f1[4 * v + 2] + f1[4 * v + 3]); k1[v].v = v;
+        k2[v].total = (unsigned)(f2[4 * v] + f2[4 * v + 1] + f2[4 * v + 2] + f2[4 * v + 3]); k2[v].v = v;
+    }
+    qsort(k1, (size_t)n, sizeof(g_key), g_cmp);
+    qsort(k2, (size_t)n, sizeof(g_key), g_cmp);
+    /* G1 lists with every entry; G2 with the last weight of each pair */
+    int *a1 = (int*)malloc(sizeof(int) * (size_t)(e1 ? e1 : 1)), *b1 = (int*)malloc(sizeof(int) * (size_t)(e1 ? e1 : 1));
+    for (long long i = 0; i < e1; i++) { a1[i] = s1[i] - 1; b1[i] = d1[i] - 1; }
+    glists g1o, g1i;
+    g_csr(n, e1, a1, b1, w1, &g1o);
+    g_csr(n, e1, b1, a1, w1, &g1i);
+    int *a2 = (int*)malloc(sizeof(int) * (size_t)(e2 ? e2 : 1)), *b2 = (int*)malloc(sizeof(int) * (size_t)(e2 ? e2 : 1));
+    int* c2 = (int*)malloc(sizeof(int) * (size_t)(e2 ? e2 : 1));
+    long long m2 = 0;
+    {
+        glists t;
+        int* s20 = (int*)malloc(sizeof(int) * (size_t)(e2 ? e2 : 1));
+        int* d20 = (int*)malloc(sizeof(int) * (size_t)(e2 ? e2 : 1));
+        for (long long i = 0; i < e2; i++) { s20[i] = s2[i] - 1; d20[i] = d2[i] - 1; }
+        g_csr(n, e2, s20, d20, w2, &t);
+        int* last = (int*)malloc(sizeof(int) * (size_t)n);
+        for (int v = 0; v < n; v++) last[v] = -1;
+        for (int u = 0; u < n; u++)
+            for (int k = t.off[u + 1] - 1; k >= t.off[u]; k--) {
+                const int v = t.id[k];
+                if (last[v] == u) continue;
+                last[v] = u;
+                a2[m2] = u; b2[m2] = v; c2[m2] = t.w[k]; m2++;
+            }
+        free(last); free(s20); free(d20); g_free(&t);
+    }
+    glists g2o, g2i;
+    g_csr(n, m2, a2, b2, c2, &g2o);
+    g_csr(n, m2, b2, a2, c2, &g2i);
+    int* m0 = (int*)malloc(sizeof(int) * (size_t)n);        /* G1 -> G2, -1 unmatched */
+    unsigned char* taken = (unsigned char*)calloc((size_t)n, 1);
+    long long* acc = (long long*)calloc((size_t)n, sizeof(long long));
+    for (int v = 0; v < n; v++) m0[v] = -1;
+    for (int i = 0; i < n; i++) {
+        const int v1 = k1[i].v;
+        for (int j = g1o.off[v1]; j < g1o.off[v1 + 1]; j++) {       /* v1 -> t */
+            const int f = m0[g1o.id[j]], w = g1o.w[j];
+            if (f < 0) continue;
+            for (int k = g2i.off[f]; k < g2i.off[f + 1]; k++) acc[g2i.id[k]] += MIN(w, g2i.w[k]);
+        }
+        for (int j = g1i.off[v1]; j < g1i.off[v1 + 1]; j++) {       /* s -> v1 */
+            const int f = m0[g1i.id[j]], w = g1i.w[j];
+            if (f < 0) continue;
+            for (int k = g2o.off[f]; k < g2o.off[f + 1]; k++) acc[g2o.id[k]] += MIN(w, g2o.w[k]);
+        }
+        double best = -INFINITY;
+        int bg = -1;
+        for (int j = 0; j < n; j++) {
+            const int v2 = k2[j].v;
+            if (taken[v2]) continue;
+            const double st = -g_distance(r1 + 4 * v1, r2 + 4 * v2);
+            const double al = (double)acc[v2];
+            const double tot = 0.3 * st + 0.7 * al;
+            if (tot > best) { best = tot; bg = v2; }
+        }
+        memset(acc, 0, sizeof(long long) * (size_t)n);
+        m0[v1] = bg;
+        if (bg >= 0) taken[bg] = 1;
+    }
+    map[0] = 0;
+    for (int v = 0; v < n; v++) map[v + 1] = m0[v] + 1;
+    free(m0); free(taken); free(acc);
+    g_free(&g1o); g_free(&g1i); g_free(&g2o); g_free(&g2i);
+    free(a1); free(b1); free(a2); free(b2); free(c2);
+    free(f1); free(f2); free(r1); free(r2); free(k1); free(k2);
 }

@@ -2,8 +2,9 @@
 
 Loads oracle/_ref/liboracle.so (the C restatement, bm_oracle.c) and, when they
 were built, the reference's own code compiled in place:
-oracle/_ref/librefgao.so (src/graph-alignment-optimized.c) and
-oracle/_ref/librefperm.so (src/permutation.c).  Only tests/, smoke() and
+oracle/_ref/librefgao.so (src/graph-alignment-optimized.c),
+oracle/_ref/librefperm.so (src/permutation.c) and oracle/_ref/librefgreedy.so
+(src/greedy-feature-match.c).  Only tests/, smoke() and
 bench.py's CPU-baseline leg import this module, as the checker.
 """
 import ctypes as C
@@ -53,6 +54,11 @@ def orc_lib():
         L.orc_sample_quad.argtypes = [vp, u64, i32, i32, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)]
         L.orc_quad_round.argtypes = [vp, vp, i32, u64, i32, i32, vp]
         L.orc_best_swap_descent.argtypes = [vp, vp, i32, vp, vp]
+        L.orc_greedy_features.argtypes = [i32, i64, vp, vp, vp]
+        L.orc_greedy_features.restype = None
+        L.orc_greedy_distance.argtypes = [vp, vp]
+        L.orc_greedy_match.argtypes = [i32, i64, vp, vp, vp, i64, vp, vp, vp, vp]
+        L.orc_greedy_match.restype = None
         _orc = L
     return _orc
 
@@ -150,6 +156,77 @@ class Oracle:
         orc_lib().orc_quad_round(self.h, _p(m), partners, seed, max_candidates, max_verify, _p(st))
         return dict(total_delta=int(st[0]), candidates=int(st[1]), scanned=int(st[2]), verified=int(st[3]),
                     committed=int(st[4]), best_delta=int(st[5]), quads=int(st[6]))
+
+
+def greedy_features(n, src, dst):
+    """[n, 4] int32: in, out, 2-hop out-reach, 2-hop in-reach (bm_oracle.c)."""
+    s, d = (np.ascontiguousarray(x, np.int32) for x in (src, dst))
+    out = np.zeros((int(n), 4), np.int32)
+    orc_lib().orc_greedy_features(int(n), len(s), _p(s), _p(d), _p(out))
+    return out
+
+
+def greedy_distance(f1, f2):
+    a, b = (np.ascontiguousarray(x, np.int32) for x in (f1, f2))
+    return orc_lib().orc_greedy_distance(_p(a), _p(b))
+
+
+def greedy_match(g):
+    """The greedy feature matcher's matching, 1-based int32[n+1]."""
+    n = int(g["n"])
+    a = [np.ascontiguousarray(g[k], np.int32) for k in ("src1", "dst1", "w1", "src2", "dst2", "w2")]
+    m = np.zeros(n + 1, np.int32)
+    orc_lib().orc_greedy_match(n, len(a[0]), _p(a[0]), _p(a[1]), _p(a[2]), len(a[3]), _p(a[3]), _p(a[4]),
+                               _p(a[5]), _p(m))
+    return m
+
+
+class RefGreedy:
+    """The reference's src/greedy-feature-match.c, compiled in place.  Graphs
+    are loaded from CSV files by the reference's own loader."""
+
+    def __init__(self):
+        L = _load("librefgreedy.so")
+        if L is None:
+            raise OSError("oracle/_ref/librefgreedy.so not built")
+        L.refgreedy_load.restype = vp
+        L.refgreedy_load.argtypes = [C.c_char_p, C.POINTER(i32)]
+        L.refgreedy_free.argtypes = [vp]
+        L.refgreedy_free.restype = None
+        L.refgreedy_node_id.argtypes = [vp, i32]
+        L.refgreedy_features.argtypes = [vp, vp]
+        L.refgreedy_features.restype = None
+        L.refgreedy_distance.argtypes = [vp, vp]
+        L.refgreedy_match.argtypes = [vp, vp, vp]
+        self.L = L
+
+    def load(self, path):
+        n = i32()
+        g = self.L.refgreedy_load(path.encode(), C.byref(n))
+        if not g:
+            raise OSError(f"reference loader failed on {path}")
+        return g, n.value
+
+    def node_ids(self, g, n):
+        return np.array([self.L.refgreedy_node_id(g, i) for i in range(n)], np.int32)
+
+    def features(self, g, n):
+        out = np.zeros((n, 6), np.int32)
+        self.L.refgreedy_features(g, _p(out))
+        return out
+
+    def distance(self, f1, f2):
+        a, b = (np.ascontiguousarray(x, np.int32) for x in (f1, f2))
+        return self.L.refgreedy_distance(_p(a), _p(b))
+
+    def match(self, g1, g2, n):
+        out = np.zeros(n, np.int32)
+        if self.L.refgreedy_match(g1, g2, _p(out)) != 0:
+            raise RuntimeError("reference match_vertices failed")
+        return out
+
+    def free(self, g):
+        self.L.refgreedy_free(g)
 
 
 class RefGAO:

@@ -101,3 +101,54 @@ def test_score_matching_prints_score(files, cfg0):
                    str(files / "in.csv")])
     O = oracle.Oracle.from_pair(g)
     assert stdout.strip().splitlines()[-1] == str(O.score(g["map0"]))
+
+
+def _oracle_table(O, m):
+    n = O.n
+    t = np.zeros((n, n), np.int32)
+    a, b = np.triu_indices(n, 1)
+    d = O.all_deltas(m)
+    t[a, b] = d
+    t[b, a] = d
+    return t
+
+
+def test_greedy_feature_match_file(files, cfg0):
+    g = cfg0
+    out = files / "greedy.csv"
+    _run([os.path.join(BIN, "greedy-feature-match"), str(files / "gm.csv"), str(files / "gf.csv"), str(out)])
+    lines = open(out).read().splitlines()
+    assert lines[0] == "Node G1,Node G2"
+    got = np.array([[int(x) for x in ln.split(",")] for ln in lines[1:]])
+    assert np.array_equal(got[:, 0], np.arange(1, g["n"] + 1))
+    assert np.array_equal(got[:, 1], oracle.greedy_match(g)[1:])
+
+
+def test_create_score_lookup_table(files, cfg0):
+    g = cfg0
+    out = files / "lookup.csv"
+    _run([os.path.join(BIN, "create-score-lookup"), str(files / "gm.csv"), str(files / "gf.csv"),
+          str(files / "in.csv"), str(out)])
+    t = np.loadtxt(out, delimiter=",", dtype=np.int64)
+    O = oracle.Oracle.from_pair(g)
+    assert np.array_equal(t, _oracle_table(O, g["map0"]).astype(np.int16).astype(np.int64))
+
+
+def test_score_lookup_descent_and_files(files, cfg0):
+    g = cfg0
+    (files / "in_lookup.csv").write_text("0\n")
+    _run([os.path.join(BIN, "score-lookup"), str(files / "gm.csv"), str(files / "gf.csv"), str(files / "in.csv"),
+          str(files / "in_lookup.csv"), str(files / "sl.csv"), str(files / "sl_lookup.csv")],
+         env={"BM_ITERATIONS": "40"})
+    lines = open(files / "sl.csv").read().splitlines()
+    assert lines[0] == "Male Node ID,Female Node ID" and len(lines) == g["n"] + 1
+    O = oracle.Oracle.from_pair(g)
+    m = g["map0"].copy()
+    O.best_swap_descent(m, 40)
+    assert np.array_equal(_read(files / "sl.csv", g["n"]), m)
+    t = np.loadtxt(files / "sl_lookup.csv", delimiter=",", dtype=np.int64)
+    assert np.array_equal(t, _oracle_table(O, m).astype(np.int16).astype(np.int64))
+    r = subprocess.run([os.path.join(BIN, "score-lookup"), str(files / "gm.csv"), str(files / "gf.csv"),
+                        str(files / "in.csv"), str(files / "missing.csv"), str(files / "x.csv"),
+                        str(files / "y.csv")], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1

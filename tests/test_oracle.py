@@ -163,3 +163,119 @@ def test_oracle_quad_round_rule(cfg0):
         assert s2 == s + st["total_delta"]
         assert sorted(m[1:]) == list(range(1, g["n"] + 1))
         s = s2
+
+
+# ---- greedy feature matcher (src/greedy-feature-match.c:527-712) ----
+
+def _write_csv(path, s, d, w):
+    with open(path, "w") as f:
+        f.write("from,to,weight\n")
+        for a, b, c in zip(s, d, w):
+            f.write(f"{int(a)},{int(b)},{int(c)}\n")
+
+
+def _greedy_graph(rng, n, e, zero_w=False, loops=True):
+    """Random graph on ids 1..n in which every id appears (a ring), with
+    repeated edges and, optionally, self-loops."""
+    s = np.concatenate([np.arange(1, n + 1), rng.integers(1, n + 1, e)])
+    d = np.concatenate([np.arange(2, n + 2) % n + 0, rng.integers(1, n + 1, e)])
+    d[:n][d[:n] == 0] = n
+    if not loops:
+        keep = s != d
+        s, d = s[keep], d[keep]
+    s = np.concatenate([s, s[:5]])            # repeated edges
+    d = np.concatenate([d, d[:5]])
+    w = np.zeros(len(s), np.int32) if zero_w else rng.integers(1, 20, len(s)).astype(np.int32)
+    return s.astype(np.int32), d.astype(np.int32), w
+
+
+def test_greedy_features_and_distance_match_reference(tmp_path):
+    try:
+        R = oracle.RefGreedy()
+    except OSError:
+        pytest.skip("reference not compiled on this machine")
+    rng = np.random.default_rng(31)
+    n = 60
+    s, d, w = _greedy_graph(rng, n, 300)
+    p = str(tmp_path / "g.csv")
+    _write_csv(p, s, d, w)
+    g, nn = R.load(p)
+    try:
+        assert nn == n and np.array_equal(R.node_ids(g, n), np.arange(1, n + 1))
+        ref = R.features(g, n)
+    finally:
+        R.free(g)
+    mine = oracle.greedy_features(n, s, d)
+    assert np.array_equal(mine, ref[:, :4])
+    assert np.array_equal(mine.sum(1), ref[:, 4])
+    for _ in range(300):
+        f1 = mine[rng.integers(n)]
+        f2 = rng.integers(0, 50, 4).astype(np.int32)
+        if f2.sum() == 0:
+            continue
+        assert oracle.greedy_distance(f1, f2) == R.distance(f1, f2)
+
+
+@pytest.mark.parametrize("seed", [5, 6, 7])
+def test_greedy_match_structural_part_matches_reference(tmp_path, seed):
+    """With every G1 weight 0 the align term vanishes in both: the
+    reference's own match_vertices then gives the oracle's matching.  (Equal
+    totals keep index order in the reference because this C library's qsort
+    is a stable merge sort; the oracle and the engine order them by id.)"""
+    try:
+        R = oracle.RefGreedy()
+    except OSError:
+        pytest.skip("reference not compiled on this machine")
+    rng = np.random.default_rng(seed)
+    n = 40
+    s1, d1, w1 = _greedy_graph(rng, n, 160, zero_w=True)
+    s2, d2, w2 = _greedy_graph(rng, n, 160)
+    p1, p2 = str(tmp_path / "g1.csv"), str(tmp_path / "g2.csv")
+    _write_csv(p1, s1, d1, w1)
+    _write_csv(p2, s2, d2, w2)
+    g1, _ = R.load(p1)
+    g2, _ = R.load(p2)
+    try:
+        ref = R.match(g1, g2, n)
+    finally:
+        R.free(g1)
+        R.free(g2)
+    mine = oracle.greedy_match(dict(n=n, src1=s1, dst1=d1, w1=w1, src2=s2, dst2=d2, w2=w2))
+    assert np.array_equal(mine[1:], ref)
+    assert sorted(mine[1:]) == list(range(1, n + 1))
+
+
+def test_greedy_match_against_python_restatement():
+    """The oracle's align term and tie rule against a plain-Python loop."""
+    rng = np.random.default_rng(9)
+    n = 30
+    s1, d1, w1 = _greedy_graph(rng, n, 120)
+    s2, d2, w2 = _greedy_graph(rng, n, 120)
+    w2[3] = 0
+    g = dict(n=n, src1=s1, dst1=d1, w1=w1, src2=s2, dst2=d2, w2=w2)
+    f1 = oracle.greedy_features(n, s1, d1)
+    f2 = oracle.greedy_features(n, s2, d2)
+    W2 = {}
+    for a, b, c in zip(s2, d2, w2):
+        W2[(int(a), int(b))] = int(c)                        # last weight wins
+    o1 = sorted(range(1, n + 1), key=lambda v: (-int(f1[v - 1].sum()), v))
+    o2 = sorted(range(1, n + 1), key=lambda v: (-int(f2[v - 1].sum()), v))
+    m = {}
+    for v1 in o1:
+        best, bg = -np.inf, None
+        for v2 in o2:
+            if v2 in m.values():
+                continue
+            al = 0
+            for a, b, c in zip(s1, d1, w1):
+                if a == v1 and b in m:
+                    al += min(int(c), W2.get((v2, m[b]), 0))
+                if b == v1 and a in m:
+                    al += min(int(c), W2.get((m[a], v2), 0))
+            st = -oracle.greedy_distance(f1[v1 - 1], f2[v2 - 1])
+            tot = 0.3 * st + 0.7 * al
+            if tot > best:
+                best, bg = tot, v2
+        m[v1] = bg
+    mine = oracle.greedy_match(g)
+    assert [mine[v] for v in range(1, n + 1)] == [m[v] for v in range(1, n + 1)]
