@@ -277,18 +277,23 @@ def run_engine(args, g, world, rank, local, pg):
         runs = {}
         for inc in (False, True):
             E.set_mapping(g["map0"])
-            tot, upd, sw = 0.0, 0, 0
+            tot, upd, sw, per = 0.0, 0, 0, []
             for _ in range(500):
                 s = E.sweep(incremental=inc)
                 tot += s["ms_total"]
                 upd += s["profit_mode"] == 1
                 sw += 1
+                per.append([s["committed"], s["profit_mode"], round(s["ms_prep"] + s["ms_hub"] + s["ms_profit"], 3),
+                            round(s["ms_total"], 3)])
                 if s["committed"] == 0:
                     break
-            runs[inc] = (tot, upd, sw, s["score_after"], E.get_mapping())
+            runs[inc] = (tot, upd, sw, s["score_after"], E.get_mapping(), per)
         assert runs[False][3] == runs[True][3] and np.array_equal(runs[False][4], runs[True][4])
         descent = {"sweeps": runs[False][2], "final_score": runs[False][3], "rebuild_ms": runs[False][0],
-                   "incremental_ms": runs[True][0], "updated_sweeps": runs[True][1]}
+                   "incremental_ms": runs[True][0], "updated_sweeps": runs[True][1],
+                   "per_sweep_incremental": runs[True][5],
+                   "per_sweep_fields": ["committed", "profit_mode (0 rebuilt, 1 updated)", "ms making S exact",
+                                        "ms sweep"]}
 
     if rank == 0:
         cpu = None
@@ -421,6 +426,115 @@ def run_triples(args, world, rank, local, pg):
                        "start_score": start_score, "step": "one 3-cycle round"},
             "rounds": [{k: s[k] for k in ("triples", "committed", "verified", "score_after", "ms_sample",
                                          "ms_eval", "ms_commit", "ms_total")} for s in stats],
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    E.close()
+
+
+def run_greedy(args, world, rank, local, pg):
+    """The greedy feature matcher on the N=18,524 pair: one step = one whole
+    initial matching (features of both graphs + the sequential matching) from
+    host edge arrays to the host matching."""
+    import bm
+    import torch
+    torch.cuda.set_device(local)
+    p = dict(WORKLOADS["n18524_e5m"])
+    p["seed"] += rank
+    g = bm.generate(bm.gen_params(**p))
+    for _ in range(args.warmup):
+        bm.greedy_match(g)
+    barrier(pg)
+    torch.cuda.synchronize()
+    dev_ms, walls = [], []
+    with Clocks(local) as clk:
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            m, st = bm.greedy_match(g)
+            walls.append(time.perf_counter() - t0)
+            dev_ms.append(st["ms_features"] + st["ms_match"])
+        torch.cuda.synchronize()
+    barrier(pg)
+    dev_s = allreduce_max(pg, sum(dev_ms) / 1e3)
+    wall_s = allreduce_max(pg, sum(walls))
+    with bm.Engine.from_pair(g) as E:
+        E.set_mapping(m)
+        greedy_score = E.score()
+        E.set_mapping(g["map0"])
+        random_score = E.score()
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import oracle
+            t0 = time.perf_counter()
+            mo = oracle.greedy_match(g)
+            cs = time.perf_counter() - t0
+            cpu = {"value": cs, "unit": "s", "cores": os.cpu_count(), "kind": "port",
+                   "sample": "one whole matching (the oracle restatement: OpenMP features, scalar matching loop); "
+                             "identical to the GPU result: " + str(bool(np.array_equal(mo, m)))}
+        line = {
+            "metric": "greedy initial matching time", "value": dev_s / args.steps, "unit": "s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dev_s / args.steps,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "int32+f64",
+            "data": "synthetic",
+            "config": {"workload": "greedy_n18524", "n": int(g["n"]), "e1": int(len(g["src1"])),
+                       "e2": int(len(g["src2"])), "step": "features of both graphs + the sequential greedy matching"},
+            "e2e": {"value": wall_s / args.steps, "unit": "s",
+                    "h2d_bytes_per_step": 4 * 3 * (len(g["src1"]) + len(g["src2"])),
+                    "d2h_bytes_per_step": 4 * int(g["n"])},
+            "greedy_score": greedy_score, "random_start_score": random_score,
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+
+
+def run_lookup(args, world, rank, local, pg):
+    """Best-swap descent on the exact table (N=18,524 pair, random start):
+    one step = one committed swap (combine, pick, swap, table update); the
+    table is built before the timed region."""
+    import bm
+    import torch
+    torch.cuda.set_device(local)
+    p = dict(WORKLOADS["n18524_e5m"])
+    p["seed"] += rank
+    g = bm.generate(bm.gen_params(**p))
+    E = bm.Engine.from_pair(g)
+    E.set_mapping(g["map0"])
+    E.lookup_descent(max(args.warmup, 1))
+    swaps = 8 * args.steps
+    barrier(pg)
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        E.timer_mark(0)
+        st = E.lookup_descent(swaps)
+        E.timer_mark(1)
+        torch.cuda.synchronize()
+    barrier(pg)
+    ms = allreduce_max(pg, E.timer_elapsed(0, 1))
+    done = st["swaps"]
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu:
+            try:
+                c = cpu_reference(g, 8.0)
+                # the reference refreshes 4N table entries per swap (update_lookup_and_heap,
+                # src/best-swap/score-lookup.c:514-537), each one calculate_swap_delta
+                per_swap = 4 * int(g["n"])
+                cpu = {"value": c["value"] / per_swap, "unit": "swaps/s", "cores": c["threads"], "kind": "reference",
+                       "sample": f"{c['rows']} seeded rows of reference deltas under OpenMP "
+                                 f"({c['value']:.3g} deltas/s) / {per_swap} deltas refreshed per swap"}
+            except OSError as e:
+                cpu = {"value": None, "unit": "swaps/s", "cores": 0, "kind": "reference", "sample": str(e)}
+        line = {
+            "metric": "exact best swaps/s", "value": world * done / (ms / 1e3), "unit": "swaps/s", "n_gpus": world,
+            "steps": done, "warmup": args.warmup, "ms_per_step": ms / max(done, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "config": {"workload": "lookup_n18524", "n": int(g["n"]),
+                       "step": "one exact best swap: pair combine over the table, pick, swap, table update"},
+            "score_before": st["score_before"], "score_after": st["score_after"],
+            "cpu_baseline": cpu,
             "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)
@@ -596,7 +710,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--workload", default="n18524_e5m",
-                    choices=sorted(WORKLOADS) + ["batch64", "triples", "quads", "learned"])
+                    choices=sorted(WORKLOADS) + ["batch64", "triples", "quads", "learned", "greedy", "lookup"])
     ap.add_argument("--train-sweeps", type=int, default=40)
     ap.add_argument("--graph", default="n18524_e5m", choices=sorted(WORKLOADS),
                     help="graph pair of the learned workload")
@@ -607,8 +721,19 @@ def main():
     args = ap.parse_args()
     world, rank, local, pg = dist_setup()
     import bm
-    if args.workload in ("batch64", "triples", "quads") or (args.workload == "learned" and args.impl == "engine"):
-        fn = {"batch64": run_batch, "triples": run_triples, "quads": run_quads, "learned": run_learned}[args.workload]
+    if args.impl == "reference" and args.workload in ("batch64", "triples", "quads", "greedy", "lookup"):
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the reference arm times the pairwise sweep "
+                              "workloads; this workload's CPU baseline is the cpu_baseline of the engine line"}),
+                  flush=True)
+        if pg is not None:
+            pg.barrier()
+            pg.destroy_process_group()
+        return
+    if args.workload in ("batch64", "triples", "quads", "greedy", "lookup") or \
+            (args.workload == "learned" and args.impl == "engine"):
+        fn = {"batch64": run_batch, "triples": run_triples, "quads": run_quads, "learned": run_learned,
+              "greedy": run_greedy, "lookup": run_lookup}[args.workload]
         fn(args, world, rank, local, pg)
         if pg is not None:
             pg.barrier()

@@ -407,7 +407,7 @@ extern "C" bm_status bm_batch_set_mappings(bm_batch* B, const int32_t* const* ma
     if (!B || !maps) return BM_E_INPUT;
     for (int i = 0; i < B->count; i++) {
         bm_status s = bm_set_mapping(B->ctx[i], maps[i]);
-        if (s) { snprintf(B->err, sizeof B->err, "instance %d: %s", i, B->ctx[i]->err); return s; }
+        if (s) { snprintf(B->err, sizeof B->err, "instance %d: %.480s", i, B->ctx[i]->err); return s; }
     }
     return BM_OK;
 }
@@ -416,7 +416,7 @@ extern "C" bm_status bm_batch_get_mappings(bm_batch* B, int32_t* const* maps) {
     if (!B || !maps) return BM_E_INPUT;
     for (int i = 0; i < B->count; i++) {
         bm_status s = bm_get_mapping(B->ctx[i], maps[i]);
-        if (s) { snprintf(B->err, sizeof B->err, "instance %d: %s", i, B->ctx[i]->err); return s; }
+        if (s) { snprintf(B->err, sizeof B->err, "instance %d: %.480s", i, B->ctx[i]->err); return s; }
     }
     return BM_OK;
 }
@@ -425,7 +425,7 @@ extern "C" bm_status bm_batch_scores(bm_batch* B, int64_t* scores) {
     if (!B || !scores) return BM_E_INPUT;
     for (int i = 0; i < B->count; i++) {
         bm_status s = bm_score(B->ctx[i], &scores[i]);
-        if (s) { snprintf(B->err, sizeof B->err, "instance %d: %s", i, B->ctx[i]->err); return s; }
+        if (s) { snprintf(B->err, sizeof B->err, "instance %d: %.480s", i, B->ctx[i]->err); return s; }
     }
     return BM_OK;
 }

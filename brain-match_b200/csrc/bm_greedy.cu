@@ -176,9 +176,10 @@ __device__ bool grid_barrier(unsigned* bar) {
 // L2-resident), then every CTA takes the best candidate of its own slice of G2, then
 // all CTAs reduce the slices' bests, each from the same published array.
 __global__ void __launch_bounds__(kGreedyThreads, 1) k_greedy(GreedyArgs a) {
-    extern __shared__ int gsm[];
-    int* map_s = gsm;                                   // n: G1 -> G2, -1 unmatched (a copy per CTA)
-    int* pos_s = map_s + a.n;                           // slice
+    extern __shared__ double4 gsm4[];
+    double4* r2_s = gsm4;                                // slice: ratios of this CTA's candidates
+    int* map_s = reinterpret_cast<int*>(r2_s + a.slice); // n: G1 -> G2, -1 unmatched (a copy per CTA)
+    int* pos_s = map_s + a.n;                            // slice
     unsigned char* taken = reinterpret_cast<unsigned char*>(pos_s + a.slice);
     __shared__ GreedyBest wbest[kGreedyThreads / 32];
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
@@ -188,19 +189,28 @@ __global__ void __launch_bounds__(kGreedyThreads, 1) k_greedy(GreedyArgs a) {
     for (int l = tid; l < a.slice; l += blockDim.x) {
         taken[l] = l < len ? 0 : 1;
         pos_s[l] = l < len ? a.pos2[base + l] : 0x7fffffff;
+        r2_s[l] = l < len ? a.ratio2[base + l] : make_double4(0.0, 0.0, 0.0, 0.0);
     }
     __syncthreads();
     const int gw = blockIdx.x * (kGreedyThreads / 32) + wid, nwarps = gridDim.x * (kGreedyThreads / 32);
+    // the head of a step -- its vertex, edge extents and this warp's first
+    // edge -- does not depend on the previous decision: it is loaded one step
+    // ahead, while the previous step's candidates are scored
+    int nv = a.order1[0], no0 = a.off1o[nv], ndout = a.off1o[nv + 1] - no0;
+    int ni0 = a.off1i[nv], ndin = a.off1i[nv + 1] - ni0;
+    int nt = 0, nwt = 0;
+    if (gw < ndout + ndin) {
+        nt = gw < ndout ? a.id1o[no0 + gw] : a.id1i[ni0 + gw - ndout];
+        nwt = gw < ndout ? a.w1o[no0 + gw] : a.w1i[ni0 + gw - ndout];
+    }
     for (int step = 0; step < a.n; step++) {
         const int par = step & 1;
-        const int v1 = a.order1[step];
+        const int v1 = nv, o0 = no0, dout = ndout, i0 = ni0, din = ndin;
         // ---- align terms: edge j of v1 to warp j of the grid, its G2 list over the lanes ----
-        const int o0 = a.off1o[v1], dout = a.off1o[v1 + 1] - o0;
-        const int i0 = a.off1i[v1], din = a.off1i[v1 + 1] - i0;
         for (int j = gw; j < dout + din; j += nwarps) {
             const bool out = j < dout;
-            const int t = out ? a.id1o[o0 + j] : a.id1i[i0 + j - dout];
-            const int w = out ? a.w1o[o0 + j] : a.w1i[i0 + j - dout];
+            const int t = j == gw ? nt : out ? a.id1o[o0 + j] : a.id1i[i0 + j - dout];
+            const int w = j == gw ? nwt : out ? a.w1o[o0 + j] : a.w1i[i0 + j - dout];
             const int f = map_s[t];
             if (f < 0 || w <= 0) continue;
             const int* off = out ? a.off2i : a.off2o;
@@ -211,15 +221,24 @@ __global__ void __launch_bounds__(kGreedyThreads, 1) k_greedy(GreedyArgs a) {
                 if (c > 0) atomicAdd(&a.acc[lid[k]], c);
             }
         }
-        if (!grid_barrier(a.bar)) return;
-        // ---- this CTA's best candidate (and acc cleared for the next step) ----
         const double4 r1 = a.ratio1[v1];
+        if (!grid_barrier(a.bar)) return;
+        if (step + 1 < a.n) {
+            nv = a.order1[step + 1];
+            no0 = a.off1o[nv]; ndout = a.off1o[nv + 1] - no0;
+            ni0 = a.off1i[nv]; ndin = a.off1i[nv + 1] - ni0;
+            if (gw < ndout + ndin) {
+                nt = gw < ndout ? a.id1o[no0 + gw] : a.id1i[ni0 + gw - ndout];
+                nwt = gw < ndout ? a.w1o[no0 + gw] : a.w1i[ni0 + gw - ndout];
+            }
+        }
+        // ---- this CTA's best candidate (and acc cleared for the next step) ----
         GreedyBest best{-1.0 / 0.0, 0x7fffffff, -1};
         for (int l = tid; l < len; l += blockDim.x) {
             const int al = __ldcg(&a.acc[base + l]);
             if (al) a.acc[base + l] = 0;
             if (taken[l]) continue;
-            const GreedyBest c{greedy_score(r1, a.ratio2[base + l], al), pos_s[l], base + l};
+            const GreedyBest c{greedy_score(r1, r2_s[l], al), pos_s[l], base + l};
             if (better(c, best)) best = c;
         }
         for (int o = 16; o; o >>= 1) {
@@ -420,7 +439,7 @@ extern "C" bm_status bm_greedy_match(int32_t n, int64_t e1, const int32_t* src1,
     GK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     int per_sm = 0;
     const int slice0 = (n + sms - 1) / sms;
-    size_t smem = (size_t)n * 4 + (size_t)slice0 * 5 + 16;
+    size_t smem = (size_t)slice0 * sizeof(double4) + (size_t)n * 4 + (size_t)slice0 * 5 + 16;
     if (smem + 4096 > (size_t)optin) {
         set_err(nullptr, "%s: n=%d needs %zu bytes of shared memory per CTA (limit %d)", fn, n, smem, optin);
         return BM_E_INPUT;
