@@ -37,6 +37,7 @@ namespace bm {
 namespace {
 
 constexpr int kGreedyThreads = 512;
+constexpr int kGreedyUnroll = 4;   // list entries a thread has in flight in the align scatter
 constexpr unsigned kGreedySpinLimit = 1u << 24;  // polls of one grid-barrier wait (~1 s)
 
 struct GreedyBest {
@@ -172,8 +173,9 @@ __device__ bool grid_barrier(unsigned* bar) {
 }
 
 // The sequential matching, one CTA per SM (cooperative launch).  Step i:
-// every warp scatters the align terms of one of v1's edges into acc (global,
-// L2-resident), then every CTA takes the best candidate of its own slice of G2, then
+// the list entries of v1's edges are spread evenly over all threads of the
+// grid, which scatter the align terms into acc (global, L2-resident), then
+// every CTA takes the best candidate of its own slice of G2, then
 // all CTAs reduce the slices' bests, each from the same published array.
 __global__ void __launch_bounds__(kGreedyThreads, 1) k_greedy(GreedyArgs a) {
     extern __shared__ double4 gsm4[];
@@ -192,34 +194,85 @@ __global__ void __launch_bounds__(kGreedyThreads, 1) k_greedy(GreedyArgs a) {
         r2_s[l] = l < len ? a.ratio2[base + l] : make_double4(0.0, 0.0, 0.0, 0.0);
     }
     __syncthreads();
-    const int gw = blockIdx.x * (kGreedyThreads / 32) + wid, nwarps = gridDim.x * (kGreedyThreads / 32);
-    // the head of a step -- its vertex, edge extents and this warp's first
-    // edge -- does not depend on the previous decision: it is loaded one step
-    // ahead, while the previous step's candidates are scored
+    typedef cub::BlockScan<int, kGreedyThreads> Scan;
+    __shared__ typename Scan::TempStorage scan_tmp;
+    __shared__ int s_pre[kGreedyThreads + 1];   // prefix of the chunk's list lengths
+    __shared__ int s_beg[kGreedyThreads];       // list start of each edge of the chunk
+    __shared__ int s_w[kGreedyThreads];         // its G1 weight, bit 31 set for an in-edge
+    const long long gt = (long long)blockIdx.x * kGreedyThreads + tid;
+    const long long gthreads = (long long)gridDim.x * kGreedyThreads;
+    // the head of a step -- its vertex, edge extents and this thread's edge of
+    // the first chunk -- does not depend on the previous decision: it is
+    // loaded one step ahead, while the previous step's candidates are scored
     int nv = a.order1[0], no0 = a.off1o[nv], ndout = a.off1o[nv + 1] - no0;
     int ni0 = a.off1i[nv], ndin = a.off1i[nv + 1] - ni0;
     int nt = 0, nwt = 0;
-    if (gw < ndout + ndin) {
-        nt = gw < ndout ? a.id1o[no0 + gw] : a.id1i[ni0 + gw - ndout];
-        nwt = gw < ndout ? a.w1o[no0 + gw] : a.w1i[ni0 + gw - ndout];
+    if (tid < ndout + ndin) {
+        nt = tid < ndout ? a.id1o[no0 + tid] : a.id1i[ni0 + tid - ndout];
+        nwt = tid < ndout ? a.w1o[no0 + tid] : a.w1i[ni0 + tid - ndout];
     }
     for (int step = 0; step < a.n; step++) {
         const int par = step & 1;
         const int v1 = nv, o0 = no0, dout = ndout, i0 = ni0, din = ndin;
-        // ---- align terms: edge j of v1 to warp j of the grid, its G2 list over the lanes ----
-        for (int j = gw; j < dout + din; j += nwarps) {
-            const bool out = j < dout;
-            const int t = j == gw ? nt : out ? a.id1o[o0 + j] : a.id1i[i0 + j - dout];
-            const int w = j == gw ? nwt : out ? a.w1o[o0 + j] : a.w1i[i0 + j - dout];
-            const int f = map_s[t];
-            if (f < 0 || w <= 0) continue;
-            const int* off = out ? a.off2i : a.off2o;
-            const int* lid = out ? a.id2i : a.id2o;
-            const int* lw = out ? a.w2i : a.w2o;
-            for (int k = off[f] + lane; k < off[f + 1]; k += 32) {
-                const int c = min(w, lw[k]);
-                if (c > 0) atomicAdd(&a.acc[lid[k]], c);
+        // ---- align terms: v1's edges in chunks of one per thread; every CTA
+        // computes the chunk's list extents, and the chunk's list entries are
+        // spread evenly over all threads of the grid ----
+        for (int c0 = 0; c0 < dout + din; c0 += kGreedyThreads) {
+            const int j = c0 + tid;
+            int beg = 0, len = 0, wv = 0;
+            if (j < dout + din) {
+                const bool out = j < dout;
+                const int t = c0 == 0 ? nt : out ? a.id1o[o0 + j] : a.id1i[i0 + j - dout];
+                const int w = c0 == 0 ? nwt : out ? a.w1o[o0 + j] : a.w1i[i0 + j - dout];
+                const int f = map_s[t];
+                if (f >= 0 && w > 0) {
+                    const int* off = out ? a.off2i : a.off2o;
+                    beg = off[f];
+                    len = off[f + 1] - beg;
+                    wv = out ? w : (w | (int)0x80000000);
+                }
             }
+            int pre, total;
+            Scan(scan_tmp).ExclusiveSum(len, pre, total);
+            s_pre[tid] = pre;
+            s_beg[tid] = beg;
+            s_w[tid] = wv;
+            if (tid == 0) s_pre[kGreedyThreads] = total;
+            __syncthreads();
+            // kGreedyUnroll items per thread at a time: their list loads are in
+            // flight together
+            for (long long q0 = gt; q0 < total; q0 += kGreedyUnroll * gthreads) {
+                int k[kGreedyUnroll], wl[kGreedyUnroll], g2[kGreedyUnroll], w2[kGreedyUnroll];
+#pragma unroll
+                for (int u = 0; u < kGreedyUnroll; u++) {
+                    const long long q = q0 + u * gthreads;
+                    k[u] = -1;
+                    wl[u] = 0;
+                    if (q < total) {
+                        int lo = 0, hi = kGreedyThreads - 1;   // last edge with s_pre <= q
+                        while (lo < hi) {
+                            const int mid = (lo + hi + 1) >> 1;
+                            if (s_pre[mid] <= q) lo = mid; else hi = mid - 1;
+                        }
+                        k[u] = s_beg[lo] + (int)(q - s_pre[lo]);
+                        wl[u] = s_w[lo];
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kGreedyUnroll; u++) {
+                    if (k[u] < 0) continue;
+                    const bool out = wl[u] >= 0;
+                    g2[u] = out ? a.id2i[k[u]] : a.id2o[k[u]];
+                    w2[u] = out ? a.w2i[k[u]] : a.w2o[k[u]];
+                }
+#pragma unroll
+                for (int u = 0; u < kGreedyUnroll; u++) {
+                    if (k[u] < 0) continue;
+                    const int c = min(wl[u] & 0x7fffffff, w2[u]);
+                    if (c > 0) atomicAdd(&a.acc[g2[u]], c);
+                }
+            }
+            __syncthreads();
         }
         const double4 r1 = a.ratio1[v1];
         if (!grid_barrier(a.bar)) return;
@@ -227,9 +280,9 @@ __global__ void __launch_bounds__(kGreedyThreads, 1) k_greedy(GreedyArgs a) {
             nv = a.order1[step + 1];
             no0 = a.off1o[nv]; ndout = a.off1o[nv + 1] - no0;
             ni0 = a.off1i[nv]; ndin = a.off1i[nv + 1] - ni0;
-            if (gw < ndout + ndin) {
-                nt = gw < ndout ? a.id1o[no0 + gw] : a.id1i[ni0 + gw - ndout];
-                nwt = gw < ndout ? a.w1o[no0 + gw] : a.w1i[ni0 + gw - ndout];
+            if (tid < ndout + ndin) {
+                nt = tid < ndout ? a.id1o[no0 + tid] : a.id1i[ni0 + tid - ndout];
+                nwt = tid < ndout ? a.w1o[no0 + tid] : a.w1i[ni0 + tid - ndout];
             }
         }
         // ---- this CTA's best candidate (and acc cleared for the next step) ----
