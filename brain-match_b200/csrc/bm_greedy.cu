@@ -27,7 +27,9 @@
 // the published slice bests -- two bounded grid barriers per step.
 #include <cub/cub.cuh>
 #include <algorithm>
+#include <cstdio>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "bm.h"
@@ -382,17 +384,18 @@ struct GreedyDev {
         }                                                                             \
     } while (0)
 
-// Validates one graph's edges and converts ids to 0-based.
+// Validates one graph's edges and converts ids to 0-based.  The message of a
+// failure goes to err (the caller records it: this may run on a helper thread).
 bm_status load_edges(const char* fn, int n, long long m, const int32_t* s, const int32_t* d, const int32_t* w,
-                     std::vector<int>& s0, std::vector<int>& d0, std::vector<int>& w0) {
-    if (m < 0 || (m > 0 && (!s || !d || !w))) { set_err(nullptr, "%s: bad edge arrays", fn); return BM_E_INPUT; }
+                     std::vector<int>& s0, std::vector<int>& d0, std::vector<int>& w0, char* err, size_t cap) {
+    if (m < 0 || (m > 0 && (!s || !d || !w))) { snprintf(err, cap, "%s: bad edge arrays", fn); return BM_E_INPUT; }
     s0.resize(m); d0.resize(m); w0.resize(m);
     for (long long i = 0; i < m; i++) {
         if (s[i] < 1 || s[i] > n || d[i] < 1 || d[i] > n) {
-            set_err(nullptr, "%s: edge %lld (%d,%d) outside 1..%d", fn, i, s[i], d[i], n);
+            snprintf(err, cap, "%s: edge %lld (%d,%d) outside 1..%d", fn, i, s[i], d[i], n);
             return BM_E_INPUT;
         }
-        if (w[i] < 0) { set_err(nullptr, "%s: edge %lld has negative weight %d", fn, i, w[i]); return BM_E_INPUT; }
+        if (w[i] < 0) { snprintf(err, cap, "%s: edge %lld has negative weight %d", fn, i, w[i]); return BM_E_INPUT; }
         s0[i] = s[i] - 1; d0[i] = d[i] - 1; w0[i] = w[i];
     }
     return BM_OK;
@@ -432,7 +435,9 @@ extern "C" bm_status bm_greedy_features(int32_t n, int64_t e, const int32_t* src
     const char* fn = "bm_greedy_features";
     if (n < 1 || !out) { set_err(nullptr, "%s: bad arguments", fn); return BM_E_INPUT; }
     std::vector<int> s0, d0, w0;
-    bm_status s = load_edges(fn, n, e, src, dst, w, s0, d0, w0);
+    char err[256];
+    bm_status s = load_edges(fn, n, e, src, dst, w, s0, d0, w0, err, sizeof err);
+    if (s) set_err(nullptr, "%s", err);
     if (s) return s;
     HostLists lo, li;
     host_csr(n, e, s0.data(), d0.data(), w0.data(), lo);
@@ -455,17 +460,26 @@ extern "C" bm_status bm_greedy_match(int32_t n, int64_t e1, const int32_t* src1,
     const char* fn = "bm_greedy_match";
     if (n < 1 || !map) { set_err(nullptr, "%s: bad arguments", fn); return BM_E_INPUT; }
     std::vector<int> s1, d1, ww1, s2, d2, ww2;
-    bm_status s = load_edges(fn, n, e1, src1, dst1, w1, s1, d1, ww1);
-    if (!s) s = load_edges(fn, n, e2, src2, dst2, w2, s2, d2, ww2);
-    if (s) return s;
+    bm_status s = BM_OK, s_2 = BM_OK;
+    char err1[256], err2[256];
+    {
+        std::thread t([&] { s_2 = load_edges(fn, n, e2, src2, dst2, w2, s2, d2, ww2, err2, sizeof err2); });
+        s = load_edges(fn, n, e1, src1, dst1, w1, s1, d1, ww1, err1, sizeof err1);
+        t.join();
+    }
+    if (s) { set_err(nullptr, "%s", err1); return s; }
+    if (s_2) { set_err(nullptr, "%s", err2); return s_2; }
+    // the six host CSRs are independent but for G2's de-duplication, which
+    // reads G2's out-lists: built on host threads side by side
     HostLists g1o, g1i, g2o, g2i, g2od, g2id;
-    host_csr(n, e1, s1.data(), d1.data(), ww1.data(), g1o);
-    host_csr(n, e1, d1.data(), s1.data(), ww1.data(), g1i);
+    std::vector<std::thread> th;
+    th.emplace_back([&] { host_csr(n, e1, s1.data(), d1.data(), ww1.data(), g1o); });
+    th.emplace_back([&] { host_csr(n, e1, d1.data(), s1.data(), ww1.data(), g1i); });
+    th.emplace_back([&] { host_csr(n, e2, d2.data(), s2.data(), ww2.data(), g2i); });
     host_csr(n, e2, s2.data(), d2.data(), ww2.data(), g2o);
-    host_csr(n, e2, d2.data(), s2.data(), ww2.data(), g2i);
     {   // G2 with one entry per (src, dst): the last weight given
-        std::vector<int> keep;
-        keep.reserve(e2);
+        std::vector<int> ks, kd, kw;
+        ks.reserve(e2); kd.reserve(e2); kw.reserve(e2);
         std::vector<int> last((size_t)n, -1);
         for (int u = 0; u < n; u++) {
             // the last occurrence of each dst in u's row (rows keep input order)
@@ -473,19 +487,15 @@ extern "C" bm_status bm_greedy_match(int32_t n, int64_t e1, const int32_t* src1,
                 const int v = g2o.id[k];
                 if (last[v] == u) continue;
                 last[v] = u;
-                keep.push_back(k);
+                ks.push_back(u); kd.push_back(v); kw.push_back(g2o.w[k]);
             }
         }
-        std::vector<int> ks(keep.size()), kd(keep.size()), kw(keep.size());
-        std::vector<int> rowof(e2);
-        for (int u = 0; u < n; u++)
-            for (int k = g2o.off[u]; k < g2o.off[u + 1]; k++) rowof[k] = u;
-        for (size_t i = 0; i < keep.size(); i++) {
-            ks[i] = rowof[keep[i]]; kd[i] = g2o.id[keep[i]]; kw[i] = g2o.w[keep[i]];
-        }
-        host_csr(n, (long long)keep.size(), ks.data(), kd.data(), kw.data(), g2od);
-        host_csr(n, (long long)keep.size(), kd.data(), ks.data(), kw.data(), g2id);
+        const long long m = (long long)ks.size();
+        std::thread t2([&] { host_csr(n, m, kd.data(), ks.data(), kw.data(), g2id); });
+        host_csr(n, m, ks.data(), kd.data(), kw.data(), g2od);
+        t2.join();
     }
+    for (auto& t : th) t.join();
     int dev = 0, sms = 0, optin = 0;
     GK(cudaGetDevice(&dev));
     GK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));

@@ -114,3 +114,34 @@ def test_cli_argument_errors_like_the_reference(tmp_path):
     r = subprocess.run([bing, "gm.csv", "gf.csv", str(tmp_path / "missing.csv"), str(tmp_path / "o.csv"),
                         "in.csv", "out.csv"], capture_output=True, text=True)
     assert r.returncode == 1 and "Error opening file" in r.stderr
+
+
+def test_new_cli_argument_errors(tmp_path):
+    """The greedy matcher and the lookup tools check their arguments and files
+    before any device work, with the reference's exit codes."""
+    import subprocess
+    from conftest import PKG
+    b = lambda name: os.path.join(PKG, "bin", name)
+    r = subprocess.run([b("greedy-feature-match"), "a.csv"], capture_output=True, text=True)
+    assert r.returncode == 1 and "Usage" in r.stderr
+    r = subprocess.run([b("greedy-feature-match"), str(tmp_path / "no1.csv"), str(tmp_path / "no2.csv"),
+                        str(tmp_path / "out.csv")], capture_output=True, text=True)
+    assert r.returncode == 1 and "Failed to load first graph" in r.stderr
+    r = subprocess.run([b("create-score-lookup"), "a", "b"], capture_output=True, text=True)
+    assert r.returncode == 1 and "Usage" in r.stderr
+    r = subprocess.run([b("score-lookup"), "a", "b", "c"], capture_output=True, text=True)
+    assert r.returncode == 1 and "Usage" in r.stderr
+    r = subprocess.run([b("score-lookup"), "gm", "gf", "in", str(tmp_path / "missing_lookup.csv"), "o", "l"],
+                       capture_output=True, text=True)
+    assert r.returncode == 1 and "Failed to load lookup file" in r.stderr
+
+
+def test_greedy_rejects_bad_edges_before_touching_the_device():
+    g = dict(n=3, src1=[1, 4], dst1=[2, 3], w1=[1, 1], src2=[1], dst2=[2], w2=[1])
+    with pytest.raises(bm.BMError) as e:
+        bm.greedy_match(g)
+    assert e.value.status == bm.BM_E_INPUT and "outside 1..3" in str(e.value)
+    g = dict(n=3, src1=[1], dst1=[2], w1=[1], src2=[1], dst2=[2], w2=[-4])
+    with pytest.raises(bm.BMError) as e:
+        bm.greedy_match(g)
+    assert e.value.status == bm.BM_E_INPUT and "negative weight" in str(e.value)
