@@ -23,7 +23,7 @@ namespace bm {
 constexpr int kHubT = 8;          // thresholds per hub
 constexpr int kHubMaxHubs = 128;  // K = 1024
 constexpr int kGemmM = 128, kGemmN = 256, kGemmKC = 128;  // tile rows, cols, K bytes per stage
-constexpr int kGemmStages = 4;
+constexpr int kGemmStages = 2;
 constexpr int kGemmThreads = 128;
 constexpr int kGemmStageBytes = (kGemmM + kGemmN) * kGemmKC;          // 48 KB
 constexpr int kGemmSmem = kGemmStages * kGemmStageBytes + 1024 + 256;  // + alignment + barriers
