@@ -545,40 +545,62 @@ bm_status stage_profit(bm_ctx* ctx) {
 template bm_status stage_profit<true>(bm_ctx*);
 template bm_status stage_profit<false>(bm_ctx*);
 
+static bm_status ensure_moved(bm_ctx* ctx) {
+    if (ctx->moved) return BM_OK;
+    CK(dalloc(ctx, &ctx->moved, (size_t)ctx->n * sizeof(int)));
+    CK(dalloc(ctx, &ctx->minfo, 4 * sizeof(int)));
+    CK(dalloc(ctx, &ctx->mwork, 3 * sizeof(unsigned long long)));
+    return BM_OK;
+}
+
+// Step 3's row path (k_terms_rows): up to 256 edge slots per moved vertex.
+template <bool W16>
+static cudaError_t launch_terms_rows(bm_ctx* ctx, const DevView<W16>& g, int count, const int* dcount, int maxd) {
+    const size_t smem = (size_t)(ctx->n + 1) * sizeof(int);
+    cudaError_t e = cudaFuncSetAttribute(k_terms_rows<W16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    dim3 grid(count, std::min(maxd, 256));
+    k_terms_rows<W16><<<grid, kIncrRowThreads, smem, ctx->st>>>(g, ctx->pS, ctx->moved, count, dcount);
+    return cudaGetLastError();
+}
+
 template <bool W16>
 bm_status stage_refresh(bm_ctx* ctx, int* mode) {
     *mode = 0;
     if (!ctx->S_exact) return stage_profit<W16>(ctx);
     const int n = ctx->n;
-    if (!ctx->moved) {
-        CK(dalloc(ctx, &ctx->moved, (size_t)n * sizeof(int)));
-        CK(dalloc(ctx, &ctx->minfo, 4 * sizeof(int)));
-        CK(dalloc(ctx, &ctx->mwork, sizeof(unsigned long long)));
+    {
+        const bm_status sm = ensure_moved(ctx);
+        if (sm) return sm;
     }
     DevView<W16> g = view<W16>(ctx);
     CK(cudaMemsetAsync(ctx->minfo, 0, 4 * sizeof(int), ctx->st));
-    CK(cudaMemsetAsync(ctx->mwork, 0, sizeof(unsigned long long), ctx->st));
+    CK(cudaMemsetAsync(ctx->mwork, 0, 3 * sizeof(unsigned long long), ctx->st));
     k_moved<W16><<<ctx->num_sms * 2, 256, 0, ctx->st>>>(g, ctx->pS, ctx->pinvS, ctx->moved, ctx->minfo, ctx->mwork);
     CK(cudaGetLastError());
     int info[4];
-    unsigned long long work = 0, full = 0;
+    unsigned long long work[3] = {0, 0, 0}, full = 0;
     CK(cudaMemcpyAsync(info, ctx->minfo, sizeof info, cudaMemcpyDeviceToHost, ctx->st));
-    CK(cudaMemcpyAsync(&work, ctx->mwork, sizeof work, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(work, ctx->mwork, sizeof work, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaMemcpyAsync(&full, ctx->work_sum, sizeof full, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     CK(cudaEventRecord(ctx->ev_hub, ctx->st));
     CK(cudaEventRecord(ctx->ev[4], ctx->st));
     const int count = info[0];
-    ctx->upd_work = (long long)work;
+    ctx->upd_work = (long long)work[2];
     if (count == 0) {
         *mode = 2;
         CK(cudaEventRecord(ctx->ev[5], ctx->st));
         return BM_OK;
     }
     // an atomic into S costs about kIncrAtomicCost shared-memory terms of a
-    // rebuild, a permuted column entry kIncrPermCost
-    const double est = kIncrAtomicCost * (double)work + kIncrPermCost * (double)n * count;
-    if (info[1] || count > kIncrMaxMoved || est >= (double)full) return stage_profit<W16>(ctx);
+    // rebuild, a row written whole kIncrRowCost per column, a permuted column
+    // entry kIncrPermCost
+    const double est = kIncrAtomicCost * (double)work[0] + kIncrRowCost * (double)n * (double)work[1] +
+                       kIncrPermCost * (double)n * count;
+    const bool rows_fit = (size_t)(n + 1) * sizeof(int) + 1024 <= ctx->smem_optin;
+    if (info[1] || count > kIncrMaxMoved || est >= (double)full || (work[1] && !rows_fit))
+        return stage_profit<W16>(ctx);
     const int maxd = std::max(info[2], 1);
     ctx->S_exact = false;
     {
@@ -597,6 +619,7 @@ bm_status stage_refresh(bm_ctx* ctx, int* mode) {
         dim3 grid(count, (maxd + kIncrEdgesPerBlock - 1) / kIncrEdgesPerBlock);
         k_terms<W16><<<grid, 256, 0, ctx->st>>>(g, ctx->pS, ctx->moved, count, nullptr);
         CK(cudaGetLastError());
+        if (work[1]) CK(launch_terms_rows<W16>(ctx, g, count, nullptr, maxd));
     }
     {
         dim3 grid(count, (maxd + kIncrCornerEdges - 1) / kIncrCornerEdges);
@@ -772,13 +795,6 @@ extern "C" bm_status bm_sweep(bm_ctx* ctx, const bm_sweep_opts* opts, bm_sweep_s
 // Exact swap-lookup table (src/best-swap/create-score-lookup.c:289-296,
 // src/best-swap/score-lookup.c:514-640): the table is the profit matrix, kept
 // exact by the moved-vertex update; the heap is the per-row best partners.
-static bm_status ensure_moved(bm_ctx* ctx) {
-    if (ctx->moved) return BM_OK;
-    CK(dalloc(ctx, &ctx->moved, (size_t)ctx->n * sizeof(int)));
-    CK(dalloc(ctx, &ctx->minfo, 4 * sizeof(int)));
-    CK(dalloc(ctx, &ctx->mwork, sizeof(unsigned long long)));
-    return BM_OK;
-}
 
 extern "C" bm_status bm_lookup_rows(bm_ctx* ctx, int32_t a0, int32_t rows, int32_t* out) {
     if (!ctx || !out || rows < 0) return BM_E_INPUT;
@@ -805,6 +821,11 @@ extern "C" bm_status bm_lookup_rows(bm_ctx* ctx, int32_t a0, int32_t rows, int32
 template <bool W16>
 static bm_status lookup_descent_impl(bm_ctx* ctx, int max_swaps, bm_lookup_stats* st) {
     const int n = ctx->n;
+    if ((size_t)(n + 1) * sizeof(int) + 1024 > ctx->smem_optin) {
+        set_err(ctx, "bm_lookup_descent: n=%d needs a %zu-byte shared-memory row (limit %zu)", n,
+                (size_t)(n + 1) * sizeof(int), ctx->smem_optin);
+        return BM_E_INPUT;
+    }
     bm_status s = ensure_S(ctx);
     if (!s) s = ensure_moved(ctx);
     if (s) return s;
@@ -835,6 +856,7 @@ static bm_status lookup_descent_impl(bm_ctx* ctx, int max_swaps, bm_lookup_stats
             k_corner<W16><<<gc, kIncrCornerEdges, 0, ctx->st>>>(g, ctx->pS, ctx->pS, ctx->moved, 2, ctx->minfo, -1);
             k_perm_cols_small<<<pblocks, 256, 0, ctx->st>>>(ctx->S, n, ctx->moved, ctx->minfo, ctx->p, ctx->pinvS);
             k_terms<W16><<<gt, 256, 0, ctx->st>>>(g, ctx->pS, ctx->moved, 2, ctx->minfo);
+            CK(launch_terms_rows<W16>(ctx, g, 2, ctx->minfo, maxd));
             k_corner<W16><<<gc, kIncrCornerEdges, 0, ctx->st>>>(g, ctx->p, ctx->pS, ctx->moved, 2, ctx->minfo, 1);
             k_sync_exact<<<1, 32, 0, ctx->st>>>(ctx->moved, ctx->minfo, ctx->p, ctx->pS, ctx->pinvS, n);
             CK(cudaGetLastError());

@@ -33,11 +33,25 @@ constexpr int kIncrCornerEdges = 128;  // G1 edges per block in the corner passe
 // column entry.
 constexpr double kIncrAtomicCost = 20.0;
 constexpr double kIncrPermCost = 16.0;
+// A G1 edge whose two G2 lists together hold at least n/4 entries changes a
+// quarter of its row: its terms are summed in shared memory first and the row
+// written once with coalesced atomics (about n/8 sectors, ~3 units per column)
+// instead of one scattered atomic per entry.
+constexpr double kIncrRowCost = 3.0;
+constexpr int kIncrRowThreads = 512;
+
+// Whether the edges of moved vertex m in one direction take the row path:
+// the two lists (old image, new image) hold >= n/4 entries together.
+__device__ __forceinline__ bool incr_heavy(const int* off, int fo, int fn, int n) {
+    return 4LL * ((off[fo + 1] - off[fo]) + (off[fn + 1] - off[fn])) >= (long long)n;
+}
 
 // Moved vertices (p != pS), compacted into moved[], with info[0] = count,
 // info[1] = 1 when a vertex took a G2 vertex that nobody held under pS (its T
 // column was never built: only a rebuild has it), info[2] = largest G1 degree
-// (in + out) among them, and *work = the list entries steps 1-4 touch.
+// (in + out) among them, work[0] = the list entries step 3 applies by single
+// atomics, work[1] = the rows it writes whole (incr_heavy), work[2] = all list
+// entries of step 3.
 template <bool W16>
 __global__ void k_moved(DevView<W16> g, const int* __restrict__ pS, const int* __restrict__ pinvS,
                         int* __restrict__ moved, int* __restrict__ info, unsigned long long* __restrict__ work) {
@@ -46,7 +60,7 @@ __global__ void k_moved(DevView<W16> g, const int* __restrict__ pS, const int* _
     for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
         const int v = base + threadIdx.x;
         bool mv = false;
-        unsigned long long w = 0;
+        unsigned long long w = 0, rows = 0, all = 0;
         int deg = 0;
         if (v < n) {
             const int fo = pS[v], fn = g.p[v];
@@ -54,10 +68,14 @@ __global__ void k_moved(DevView<W16> g, const int* __restrict__ pS, const int* _
                 mv = true;
                 if (fn != n && pinvS[fn] == n) info[1] = 1;
                 const int di = g.off1i[v + 1] - g.off1i[v], dout = g.off1o[v + 1] - g.off1o[v];
-                w = (unsigned long long)di * (unsigned long long)((g.off2i[fo + 1] - g.off2i[fo]) +
-                                                                  (g.off2i[fn + 1] - g.off2i[fn])) +
-                    (unsigned long long)dout * (unsigned long long)((g.off2o[fo + 1] - g.off2o[fo]) +
-                                                                    (g.off2o[fn + 1] - g.off2o[fn]));
+                const unsigned long long ei = (unsigned long long)di *
+                    (unsigned long long)((g.off2i[fo + 1] - g.off2i[fo]) + (g.off2i[fn + 1] - g.off2i[fn]));
+                const unsigned long long eo = (unsigned long long)dout *
+                    (unsigned long long)((g.off2o[fo + 1] - g.off2o[fo]) + (g.off2o[fn + 1] - g.off2o[fn]));
+                const bool hi = incr_heavy(g.off2i, fo, fn, n), ho = incr_heavy(g.off2o, fo, fn, n);
+                w = (hi ? 0ull : ei) + (ho ? 0ull : eo);
+                rows = (hi ? (unsigned long long)di : 0ull) + (ho ? (unsigned long long)dout : 0ull);
+                all = ei + eo;
                 deg = di + dout;
             }
         }
@@ -70,10 +88,14 @@ __global__ void k_moved(DevView<W16> g, const int* __restrict__ pS, const int* _
         if (mv) moved[slot + __popc(bal & ((1u << lane) - 1u))] = v;
         for (int o = 16; o; o >>= 1) {
             w += __shfl_xor_sync(0xffffffffu, w, o);
+            rows += __shfl_xor_sync(0xffffffffu, rows, o);
+            all += __shfl_xor_sync(0xffffffffu, all, o);
             deg = max(deg, __shfl_xor_sync(0xffffffffu, deg, o));
         }
         if (lane == 0) {
-            atomicAdd(work, w);
+            atomicAdd(&work[0], w);
+            atomicAdd(&work[1], rows);
+            atomicAdd(&work[2], all);
             atomicMax(&info[2], deg);
         }
     }
@@ -155,9 +177,11 @@ __global__ void __launch_bounds__(256) k_terms(DevView<W16> g, const int* __rest
     const int so = g.off1o[m], lo = g.off1o[m + 1] - so;
     const int si = g.off1i[m], li = g.off1i[m + 1] - si;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const bool hi = incr_heavy(g.off2i, fo, fn, n), ho = incr_heavy(g.off2o, fo, fn, n);
     for (int t = wid; t < kIncrEdgesPerBlock; t += 8) {
         const int j = blockIdx.y * kIncrEdgesPerBlock + t;
         if (j >= lo + li) break;
+        if (j < li ? hi : ho) continue;  // k_terms_rows takes it
         int row, w1;
         const int* off;
         const E* list;
@@ -184,12 +208,67 @@ __global__ void __launch_bounds__(256) k_terms(DevView<W16> g, const int* __rest
     }
 }
 
+// Step 3 for the edges whose lists cover much of their row (incr_heavy): a
+// block per edge sums its terms in a shared-memory row, then adds the nonzero
+// entries to S in column order.  grid = (count, up to 256 edge slots per
+// moved vertex), dynamic shared memory (n+1) ints.
+template <bool W16>
+__global__ void __launch_bounds__(kIncrRowThreads) k_terms_rows(DevView<W16> g, const int* __restrict__ pS,
+                                                               const int* __restrict__ moved, int count,
+                                                               const int* __restrict__ dcount) {
+    typedef Ent<W16> EN;
+    typedef typename EN::T E;
+    extern __shared__ int rowbuf[];
+    if (dcount) count = min(count, *dcount);
+    if ((int)blockIdx.x >= count) return;
+    const int n = g.n;
+    const int m = moved[blockIdx.x];
+    const int fo = pS[m], fn = g.p[m];
+    const bool hi = incr_heavy(g.off2i, fo, fn, n), ho = incr_heavy(g.off2o, fo, fn, n);
+    if (!hi && !ho) return;
+    const int so = g.off1o[m], lo = g.off1o[m + 1] - so;
+    const int si = g.off1i[m], li = g.off1i[m + 1] - si;
+    const int j0 = hi ? 0 : li, j1 = ho ? li + lo : li;
+    if (j0 + (int)blockIdx.y >= j1) return;
+    for (int c = threadIdx.x; c <= n; c += blockDim.x) rowbuf[c] = 0;
+    for (int j = j0 + blockIdx.y; j < j1; j += gridDim.y) {
+        int row, w1;
+        const int* off;
+        const E* list;
+        if (j < li) {
+            const E e = g.ent1i[si + j];
+            row = EN::id(e); w1 = EN::w(e);
+            off = g.off2i; list = g.ent2i;
+        } else {
+            const E e = g.ent1o[so + (j - li)];
+            row = EN::id(e); w1 = EN::w(e);
+            off = g.off2o; list = g.ent2o;
+        }
+        __syncthreads();
+        for (int k = off[fo] + threadIdx.x; k < off[fo + 1]; k += blockDim.x) {
+            const E e = list[k];
+            atomicAdd(&rowbuf[g.pinv[EN::id(e)]], -imin(w1, EN::w(e)));   // column n: unmatched, dropped
+        }
+        for (int k = off[fn] + threadIdx.x; k < off[fn + 1]; k += blockDim.x) {
+            const E e = list[k];
+            atomicAdd(&rowbuf[g.pinv[EN::id(e)]], imin(w1, EN::w(e)));
+        }
+        __syncthreads();
+        int* srow = g.S + (size_t)row * n;
+        for (int c = threadIdx.x; c < n; c += blockDim.x) {
+            const int v = rowbuf[c];
+            if (v) { atomicAdd(&srow[c], v); rowbuf[c] = 0; }
+        }
+        if (threadIdx.x == 0) rowbuf[n] = 0;
+    }
+}
+
 }  // namespace bm
 
 namespace bm {
 
-constexpr int kSmallMoved = 4;
-constexpr int kLookupBatch = 32;  // best-swap steps enqueued between host checks  // moved vertices of the thread-per-row column permutation
+constexpr int kSmallMoved = 4;    // moved vertices of the thread-per-row column permutation
+constexpr int kLookupBatch = 32;  // best-swap steps enqueued between host checks
 
 // Step 2 for at most kSmallMoved moved vertices (*dcount of them): one thread per row.
 __global__ void k_perm_cols_small(int* __restrict__ S, int n, const int* __restrict__ moved,

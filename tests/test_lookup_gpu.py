@@ -143,3 +143,31 @@ def test_best_swap_descent_to_convergence_with_unmatched_vertices():
         # a second call has nothing to do
         st2 = E.lookup_descent(10)
         assert st2["swaps"] == 0 and st2["converged"] == 1 and st2["refresh_mode"] == 2
+
+
+@pytest.mark.parametrize("flags", [0, bm.BM_FLAG_FORCE_I32])
+def test_dense_graph_row_path_identical(flags):
+    """A dense pair (average degree 100 in each direction, n = 600): the two
+    G2 lists of almost every moved vertex cover a quarter of its row, so the
+    update sums each edge's terms in shared memory and writes the row whole.
+    Sweeps and the best-swap descent must still equal the oracle."""
+    g = bm.generate(bm.gen_params(n=600, e=60000, seed=23))
+    O = _oracle(g)
+    m = g["map0"].copy()
+    with _engine(g, flags) as E:
+        E.set_mapping(m)
+        modes = []
+        for _ in range(60):
+            st = E.sweep(incremental=True)
+            O.sweep(m)
+            modes.append(st["profit_mode"])
+            assert np.array_equal(E.get_mapping(), m)
+            if st["committed"] == 0:
+                break
+        assert np.array_equal(E.lookup_rows(1, 600), _table(O, m))
+        m2 = g["map0"].copy()
+        E.set_mapping(m2)
+        st = E.lookup_descent(60)
+        O.best_swap_descent(m2, 60)
+        assert np.array_equal(E.get_mapping(), m2) and E.score() == O.score(m2) == st["score_after"]
+        assert np.array_equal(E.lookup_rows(1, 600), _table(O, m2))
