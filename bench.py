@@ -250,7 +250,7 @@ def run_engine(args, g, world, rank, local, pg):
         except (OSError, ValueError):
             traffic = None
     terms = statistics.mean(s["min_terms"] for s in stats)
-    # the survey's whole-sweep roofline: T_roof = max(compulsory bytes / HBM peak,
+    # the whole-sweep roofline: T_roof = max(compulsory bytes / HBM peak,
     # algorithmic min+add / INT32 peak), with the reference's per-delta work
     # 2 (d(a) + d(b)) summed over all pairs = 4 E (N - 1); the INT32 peak is
     # measured live by the engine's microbenchmark (independent min+add pairs)
