@@ -28,12 +28,27 @@ __device__ __forceinline__ void combine_tile(const int* __restrict__ S, int n, i
     __shared__ unsigned long long cpart[8][T];
     const int a0 = ti * T, b0 = tj * T;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;  // 8 warps
-    for (int i = tid; i < T * T; i += 256) {
-        const int r = i / T, c = i % T;
-        const int a = a0 + r, b = b0 + c;
-        sA[r][c] = (a < n && b < n) ? S[(size_t)a * n + b] : 0;
-        const int bb = b0 + r, aa = a0 + c;
-        sB[r][c] = (bb < n && aa < n) ? S[(size_t)bb * n + aa] : 0;
+    if ((n & 3) == 0) {
+        // 16-byte streaming loads: with n a multiple of 4 every 4-column group
+        // of a row is aligned and lies wholly inside or outside the matrix
+        for (int i = tid; i < T * T / 4; i += 256) {
+            const int r = i / (T / 4), c = (i % (T / 4)) * 4;
+            const int a = a0 + r, b = b0 + c;
+            const int bb = b0 + r, aa = a0 + c;
+            int4 va = make_int4(0, 0, 0, 0), vb = make_int4(0, 0, 0, 0);
+            if (a < n && b < n) va = __ldcs(reinterpret_cast<const int4*>(S + (size_t)a * n + b));
+            if (bb < n && aa < n) vb = __ldcs(reinterpret_cast<const int4*>(S + (size_t)bb * n + aa));
+            sA[r][c] = va.x; sA[r][c + 1] = va.y; sA[r][c + 2] = va.z; sA[r][c + 3] = va.w;
+            sB[r][c] = vb.x; sB[r][c + 1] = vb.y; sB[r][c + 2] = vb.z; sB[r][c + 3] = vb.w;
+        }
+    } else {
+        for (int i = tid; i < T * T; i += 256) {
+            const int r = i / T, c = i % T;
+            const int a = a0 + r, b = b0 + c;
+            sA[r][c] = (a < n && b < n) ? S[(size_t)a * n + b] : 0;
+            const int bb = b0 + r, aa = a0 + c;
+            sB[r][c] = (bb < n && aa < n) ? S[(size_t)bb * n + aa] : 0;
+        }
     }
     if (tid < T) {
         const int a = a0 + tid, b = b0 + tid;
