@@ -265,3 +265,20 @@ def test_commit_across_ctas_is_identical(cfg0, flags):
         for _ in range(4):
             orc.sweep(m, max_verify=max_verify)
         np.testing.assert_array_equal(maps[0], m)
+
+
+def test_sweeps_at_n_26000_match_oracle():
+    """A pair larger than the benchmark's (n = 26,000, sparse): the set
+    commit's per-vertex state still fits one CTA's shared memory, and the
+    sweeps make the oracle's moves."""
+    g = bm.generate(bm.gen_params(n=26000, e=60000, seed=29))
+    O = _oracle(g)
+    m = g["map0"].copy()
+    with _engine(g) as E:
+        E.set_mapping(m)
+        for _ in range(2):
+            st = E.sweep()
+            ost = O.sweep(m)
+            assert st["committed"] == ost["committed"] > 0
+            assert np.array_equal(E.get_mapping(), m)
+        assert E.score() == O.score(m)
