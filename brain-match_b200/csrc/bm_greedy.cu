@@ -22,9 +22,10 @@
 //
 // The sequential loop runs as one cooperative grid, a CTA per SM: each step
 // scatters the align terms through the G2 lists of the matched neighbours'
-// images into an L2-resident array (the edges spread over the CTAs), every
-// CTA takes the best of its own slice of candidates, and every CTA reduces
-// the published slice bests -- two bounded grid barriers per step.
+// images into an L2-resident array (the list entries spread evenly over all
+// threads of the grid), every CTA takes the best of its own slice of
+// candidates, and every CTA reduces the published slice bests -- two bounded
+// grid barriers per step.
 #include <cub/cub.cuh>
 #include <algorithm>
 #include <cstdio>
