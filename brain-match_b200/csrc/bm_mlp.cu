@@ -33,6 +33,9 @@
 namespace {
 
 constexpr int kFeat = 32;
+// exhaustive sweeps of the learned paths keep the profit matrix exact across
+// commits (updated from the moved vertices where that is cheaper): same moves
+const bm_sweep_opts kIncremental = {0, -1, 0, 1, {0, 0, 0, 0}};
 // parameter layout (fp32): W1[256x128] b1[256] W2[256x256] b2[256] w3[256] b3[1]
 constexpr int oW1 = 0, oB1 = oW1 + kMlpHid * kMlpIn, oW2 = oB1 + kMlpHid, oB2 = oW2 + kMlpHid * kMlpHid,
               oW3 = oB2 + kMlpHid, oB3 = oW3 + kMlpHid, kParams = oB3 + 1;
@@ -753,7 +756,8 @@ static bm_status train_from_impl(bm_mlp* M, bm_ctx* ctx, int sweeps, int extra, 
     //    row bests), the samples, the features; then one ordinary sweep
     for (int sw = 0; sw < sweeps; sw++) {
         if ((s = ensure_S(ctx))) return s;
-        if ((s = stage_profit<W16>(ctx))) return s;
+        int mode = 0;
+        if ((s = stage_refresh<W16>(ctx, &mode))) return s;
         if ((s = stage_combine(ctx, nullptr))) return s;
         if ((s = features<W16>(ctx, M))) return s;
         k_samples<W16><<<(n + 255) / 256, 256, 0, M->cs>>>(view<W16>(ctx), ctx->rowbest, extra,
@@ -765,7 +769,7 @@ static bm_status train_from_impl(bm_mlp* M, bm_ctx* ctx, int sweeps, int extra, 
         MK(cudaMemcpyAsync(M->ps.as<int>() + (size_t)n * sw, ctx->p, (size_t)n * sizeof(int),
                            cudaMemcpyDeviceToDevice, M->cs));
         bm_sweep_stats st;
-        if ((s = bm_sweep(ctx, nullptr, &st))) { snprintf(M->err, sizeof M->err, "%s", ctx->err); return s; }
+        if ((s = bm_sweep(ctx, &kIncremental, &st))) { snprintf(M->err, sizeof M->err, "%s", ctx->err); return s; }
     }
     // 2. train: epochs of SGD over all logged samples, freshly shuffled each epoch
     double* eacc = M->eacc.as<double>();
@@ -937,7 +941,7 @@ static bm_status learned_impl(bm_ctx* ctx, bm_mlp* M, const bm_learned_opts* o, 
     if (cs.committed == 0 && allow_fallback) {  // nothing improving among the proposals: exhaustive sweep
         *fell_back = 1;
         bm_sweep_stats fs;
-        r = bm_sweep(ctx, nullptr, &fs);
+        r = bm_sweep(ctx, &kIncremental, &fs);
         if (r) { snprintf(M->err, sizeof M->err, "%s", ctx->err); return r; }
         if (stats) {
             stats->score_after = fs.score_after;
@@ -997,7 +1001,7 @@ extern "C" bm_status bm_learned_run(bm_ctx* ctx, bm_mlp* M, const bm_learned_opt
         if (!learned || st.committed == 0) {  // exhaustive sweep (also the fallback of a fruitless learned one)
             const long long before = ctx->score;
             bm_sweep_stats fs;
-            s = bm_sweep(ctx, nullptr, &fs);
+            s = bm_sweep(ctx, &kIncremental, &fs);
             if (s) { snprintf(M->err, sizeof M->err, "%s", ctx->err); break; }
             rate_full = (double)(fs.score_after - before) / std::max(fs.ms_total, 1e-3f);
             rs.exhaustive++;
