@@ -405,6 +405,7 @@ def run_triples(args, world, rank, local, pg):
     start_score = E.score()
     for r in range(args.warmup):
         E.triple_round(partners=256, seed=1000 + r)
+    m_timed = E.get_mapping()
     barrier(pg)
     torch.cuda.synchronize()
     stats = []
@@ -416,6 +417,10 @@ def run_triples(args, world, rank, local, pg):
         torch.cuda.synchronize()
     barrier(pg)
     ms = allreduce_max(pg, E.timer_elapsed(0, 1))
+    m_end = E.get_mapping()
+    inc_ms = replay_rounds_incremental(
+        E, m_timed, args.steps, lambda r, inc: E.triple_round(partners=256, seed=2000 + r, incremental=inc))
+    assert np.array_equal(E.get_mapping(), m_end)
     rot = sum(s["rotations"] for s in stats)
     if rank == 0:
         line = {
@@ -424,12 +429,32 @@ def run_triples(args, world, rank, local, pg):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
             "config": {"workload": "triples_n18524", "partners": 256, "pre_sweeps": args.pre_sweeps,
                        "start_score": start_score, "step": "one 3-cycle round"},
+            "incremental": {"ms_per_step": inc_ms, "value": world * rot / (args.steps * inc_ms / 1e3),
+                            "note": "the same rounds with the profit matrix updated from the previous "
+                                    "round's moves (identical moves, asserted)"},
             "rounds": [{k: s[k] for k in ("triples", "committed", "verified", "score_after", "ms_sample",
                                          "ms_eval", "ms_commit", "ms_total")} for s in stats],
             "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)
     E.close()
+
+
+def replay_rounds_incremental(E, start, steps, round_fn):
+    """The timed rounds replayed from the same matching with the profit matrix
+    updated from the previous round's moves instead of rebuilt; the moves must
+    be identical.  Returns the device ms per round."""
+    import torch
+    E.set_mapping(start)
+    round_fn(0, True)      # the first round after a new mapping rebuilds: untimed
+    E.set_mapping(start)
+    torch.cuda.synchronize()
+    E.timer_mark(2)
+    for r in range(steps):
+        round_fn(r, True)
+    E.timer_mark(3)
+    torch.cuda.synchronize()
+    return E.timer_elapsed(2, 3) / steps
 
 
 def run_greedy(args, world, rank, local, pg):
@@ -560,6 +585,7 @@ def run_quads(args, world, rank, local, pg):
     start_score = E.score()
     for r in range(args.warmup):
         E.quad_round(partners=64, seed=1000 + r)
+    m_timed = E.get_mapping()
     barrier(pg)
     torch.cuda.synchronize()
     stats = []
@@ -571,6 +597,10 @@ def run_quads(args, world, rank, local, pg):
         torch.cuda.synchronize()
     barrier(pg)
     ms = allreduce_max(pg, E.timer_elapsed(0, 1))
+    m_end = E.get_mapping()
+    inc_ms = replay_rounds_incremental(
+        E, m_timed, args.steps, lambda r, inc: E.quad_round(partners=64, seed=2000 + r, incremental=inc))
+    assert np.array_equal(E.get_mapping(), m_end)
     perms = sum(s["permutations"] for s in stats)
     if rank == 0:
         line = {
@@ -580,6 +610,9 @@ def run_quads(args, world, rank, local, pg):
             "dtype": "int32", "data": "synthetic",
             "config": {"workload": "quads_n18524", "partners": 64, "pre_sweeps": args.pre_sweeps,
                        "start_score": start_score, "step": "one 4-set round (23 permutations per set)"},
+            "incremental": {"ms_per_step": inc_ms, "value": world * perms / (args.steps * inc_ms / 1e3),
+                            "note": "the same rounds with the profit matrix updated from the previous "
+                                    "round's moves (identical moves, asserted)"},
             "rounds": [{k: s[k] for k in ("quads", "committed", "verified", "score_after", "ms_sample",
                                          "ms_eval", "ms_commit", "ms_total")} for s in stats],
             "clocks": clk.summary(),

@@ -48,7 +48,7 @@ class SweepStats(C.Structure):
 
 class TripleOpts(C.Structure):
     _fields_ = [("partners", C.c_int32), ("max_candidates", C.c_int32), ("max_verify", C.c_int32),
-                ("reserved0", C.c_int32), ("seed", C.c_uint64), ("reserved", C.c_int32 * 4)]
+                ("incremental", C.c_int32), ("seed", C.c_uint64), ("reserved", C.c_int32 * 4)]
 
 
 class TripleStats(C.Structure):
@@ -87,7 +87,7 @@ class LearnedRunStats(C.Structure):
 
 class QuadOpts(C.Structure):
     _fields_ = [("partners", C.c_int32), ("max_candidates", C.c_int32), ("max_verify", C.c_int32),
-                ("reserved0", C.c_int32), ("seed", C.c_uint64), ("reserved", C.c_int32 * 4)]
+                ("incremental", C.c_int32), ("seed", C.c_uint64), ("reserved", C.c_int32 * 4)]
 
 
 class QuadStats(C.Structure):
@@ -342,15 +342,16 @@ class Engine:
         _check(lib().bm_quad_deltas(self.h, len(sets), _p(sets), _p(perms), _p(out)), self.h)
         return out
 
-    def quad_round(self, partners=64, seed=0, max_candidates=0, max_verify=-1):
-        o = QuadOpts(partners, max_candidates, max_verify, 0, seed)
+    def quad_round(self, partners=64, seed=0, max_candidates=0, max_verify=-1, incremental=False):
+        o = QuadOpts(partners, max_candidates, max_verify, int(bool(incremental)), seed)
         s = QuadStats()
         _check(lib().bm_quad_round(self.h, C.byref(o), C.byref(s)), self.h)
         return {k: getattr(s, k) for k, _ in QuadStats._fields_ if k != "reserved"}
 
-    def triple_round(self, partners=256, seed=0, max_candidates=0, max_verify=-1):
+    def triple_round(self, partners=256, seed=0, max_candidates=0, max_verify=-1, incremental=False):
         o = TripleOpts()
         o.partners, o.max_candidates, o.max_verify, o.seed = partners, max_candidates, max_verify, seed
+        o.incremental = int(bool(incremental))
         s = TripleStats()
         _check(lib().bm_triple_round(self.h, C.byref(o), C.byref(s)), self.h)
         return {k: getattr(s, k) for k, _ in TripleStats._fields_ if k != "reserved"}

@@ -26,6 +26,7 @@ int main(int argc, char** argv) {
     memset(&o, 0, sizeof o);
     o.partners = (int)env_long("BM_PARTNERS", 256);
     o.max_verify = -1;
+    o.incremental = (int)env_long("BM_INCREMENTAL", 1);
     unsigned long long seed = (unsigned long long)env_long("BM_SEED", 20261205);
     for (long r = 0; r < rounds; r++) {
         long long c = cli_sweeps(&j, 1000000, 0);

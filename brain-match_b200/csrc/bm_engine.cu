@@ -1018,7 +1018,8 @@ static bm_status triple_round_impl(bm_ctx* ctx, const bm_triple_opts* o, bm_trip
     if (!ctx->tcount) CK(dalloc(ctx, &ctx->tcount, 2 * sizeof(unsigned long long)));
     const long long before = ctx->score;
     CK(cudaEventRecord(ctx->ev[0], ctx->st));
-    s = stage_profit<W16>(ctx);
+    int mode = 0;
+    s = (o && o->incremental) ? stage_refresh<W16>(ctx, &mode) : stage_profit<W16>(ctx);
     if (s) return s;
     CK(cudaEventRecord(ctx->ev[1], ctx->st));
     CK(cudaMemsetAsync(ctx->tcount, 0, 2 * sizeof(unsigned long long), ctx->st));
@@ -1118,7 +1119,8 @@ static bm_status quad_round_impl(bm_ctx* ctx, const bm_quad_opts* o, bm_quad_sta
     if (!ctx->tcount) CK(dalloc(ctx, &ctx->tcount, 2 * sizeof(unsigned long long)));
     const long long before = ctx->score;
     CK(cudaEventRecord(ctx->ev[0], ctx->st));
-    s = stage_profit<W16>(ctx);
+    int mode = 0;
+    s = (o && o->incremental) ? stage_refresh<W16>(ctx, &mode) : stage_profit<W16>(ctx);
     if (s) return s;
     CK(cudaEventRecord(ctx->ev[1], ctx->st));
     CK(cudaMemsetAsync(ctx->tcount, 0, 2 * sizeof(unsigned long long), ctx->st));

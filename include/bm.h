@@ -300,7 +300,8 @@ typedef struct {
     int32_t partners;        /* 2-hop samples per vertex (256)            */
     int32_t max_candidates;  /* sorted candidates scanned (<=0: all)      */
     int32_t max_verify;      /* re-verifications (<0: all)                */
-    int32_t reserved0;
+    int32_t incremental;     /* 1: keep the profit matrix exact across rounds
+                                (as bm_sweep_opts.incremental); same moves   */
     uint64_t seed;           /* round seed for the 2-hop sampler          */
     int32_t reserved[4];
 } bm_triple_opts;
@@ -339,7 +340,7 @@ typedef struct {
     int32_t partners;        /* 3-step walk samples per vertex (64, at most 2048) */
     int32_t max_candidates;  /* sorted candidates scanned (<=0: all)              */
     int32_t max_verify;      /* re-verifications (<0: all)                        */
-    int32_t reserved0;
+    int32_t incremental;     /* as in bm_triple_opts                       */
     uint64_t seed;           /* round seed for the sampler                        */
     int32_t reserved[4];
 } bm_quad_opts;

@@ -171,3 +171,29 @@ def test_dense_graph_row_path_identical(flags):
         O.best_swap_descent(m2, 60)
         assert np.array_equal(E.get_mapping(), m2) and E.score() == O.score(m2) == st["score_after"]
         assert np.array_equal(E.lookup_rows(1, 600), _table(O, m2))
+
+
+@pytest.mark.parametrize("flags", [0, bm.BM_FLAG_FORCE_I32])
+def test_incremental_triple_and_quad_rounds_match_oracle(cfg0, flags):
+    """3-cycle and 4-set rounds that update the profit matrix from the
+    previous round's moves make the oracle's moves, round after round."""
+    g = cfg0
+    O = _oracle(g)
+    m = g["map0"].copy()
+    with _engine(g, flags) as E:
+        E.set_mapping(m)
+        for _ in range(4):
+            E.sweep(incremental=True)
+            O.sweep(m)
+        modes = []
+        for r in range(4):
+            st = E.triple_round(partners=64, seed=40 + r, incremental=True)
+            ost = O.triple_round(m, partners=64, seed=40 + r)
+            assert st["committed"] == ost["committed"]
+            assert np.array_equal(E.get_mapping(), m)
+            st = E.quad_round(partners=32, seed=80 + r, incremental=True)
+            ost = O.quad_round(m, partners=32, seed=80 + r)
+            assert st["committed"] == ost["committed"]
+            assert np.array_equal(E.get_mapping(), m)
+        assert E.score() == O.score(m)
+        assert np.array_equal(E.lookup_rows(1, int(g["n"])), _table(O, m))
