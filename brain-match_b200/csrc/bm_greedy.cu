@@ -24,8 +24,10 @@
 // scatters the align terms through the G2 lists of the matched neighbours'
 // images into an L2-resident array (the list entries spread evenly over all
 // threads of the grid), every CTA takes the best of its own slice of
-// candidates, and every CTA reduces the published slice bests -- two bounded
-// grid barriers per step.
+// candidates, and every CTA reduces the published slice bests -- one bounded
+// grid barrier per step (the scatter of step i+1 runs before step i's decision
+// is reduced: only edges to step i's vertex need it, and those are added per
+// slice afterwards).
 #include <cub/cub.cuh>
 #include <algorithm>
 #include <cstdio>
@@ -41,6 +43,7 @@ namespace {
 
 constexpr int kGreedyThreads = 512;
 constexpr int kGreedyUnroll = 4;   // list entries a thread has in flight in the align scatter
+constexpr int kGreedyMaxFix = 32;  // edges to the previous step's vertex recorded (more: rescanned)
 constexpr unsigned kGreedySpinLimit = 1u << 24;  // polls of one grid-barrier wait (~1 s)
 
 struct GreedyBest {
@@ -120,7 +123,7 @@ struct GreedyArgs {
     const int* order1;                                    // G1 in feature order
     const int* pos2;                                      // G2 vertex -> place in feature order
     const double4 *ratio1, *ratio2;
-    int* acc;                                             // n align sums, zero between steps
+    int* acc;                                             // [2][n] align sums by step parity, zero between uses
     GreedyBest* bests;                                    // [2][gridDim.x] per-CTA bests
     unsigned* bar;                                        // [0] arrivals [1] generation [2] error
     int* map;                                             // out: G1 -> G2 (0-based)
@@ -175,6 +178,37 @@ __device__ bool grid_barrier(unsigned* bar) {
     return s_ok != 0;
 }
 
+// The grid's best of a step, reduced by every CTA from the published slice
+// bests (buffer par): v's image in map_s, the candidate taken if it is in this
+// CTA's slice [base, base + len), the output by CTA 0.  All threads call it.
+__device__ void greedy_decide(const GreedyArgs& a, int par, int v, int* map_s, unsigned char* taken, int base,
+                              int len, GreedyBest* wbest) {
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    GreedyBest best{-1.0 / 0.0, 0x7fffffff, -1};
+    for (int r = tid; r < (int)gridDim.x; r += blockDim.x) {
+        const GreedyBest* src = a.bests + par * gridDim.x + r;
+        const GreedyBest c{__ldcg(&src->score), __ldcg(&src->pos), __ldcg(&src->g)};
+        if (better(c, best)) best = c;
+    }
+    for (int o = 16; o; o >>= 1) {
+        GreedyBest y;
+        y.score = __shfl_xor_sync(0xffffffffu, best.score, o);
+        y.pos = __shfl_xor_sync(0xffffffffu, best.pos, o);
+        y.g = __shfl_xor_sync(0xffffffffu, best.g, o);
+        if (better(y, best)) best = y;
+    }
+    if (lane == 0) wbest[wid] = best;
+    __syncthreads();
+    if (tid == 0) {
+        for (int w = 1; w < kGreedyThreads / 32; w++)
+            if (better(wbest[w], best)) best = wbest[w];
+        map_s[v] = best.g;
+        if (best.g >= base && best.g < base + len) taken[best.g - base] = 1;
+        if (blockIdx.x == 0) a.map[v] = best.g;
+    }
+    __syncthreads();
+}
+
 // The sequential matching, one CTA per SM (cooperative launch).  Step i:
 // the list entries of v1's edges are spread evenly over all threads of the
 // grid, which scatter the align terms into acc (global, L2-resident), then
@@ -214,12 +248,21 @@ __global__ void __launch_bounds__(kGreedyThreads, 1) k_greedy(GreedyArgs a) {
         nt = tid < ndout ? a.id1o[no0 + tid] : a.id1i[ni0 + tid - ndout];
         nwt = tid < ndout ? a.w1o[no0 + tid] : a.w1i[ni0 + tid - ndout];
     }
+    // the edges of a step's vertex to the previous step's vertex (whose image is
+    // decided only after this step's scatter): their indices, then their terms
+    // added per slice once the image is known
+    __shared__ int s_nfix, s_fix[kGreedyMaxFix];
+    if (tid == 0) s_nfix = 0;
+    __syncthreads();
+    int prev = -1;
     for (int step = 0; step < a.n; step++) {
         const int par = step & 1;
+        int* acc = a.acc + (size_t)par * a.n;
         const int v1 = nv, o0 = no0, dout = ndout, i0 = ni0, din = ndin;
         // ---- align terms: v1's edges in chunks of one per thread; every CTA
         // computes the chunk's list extents, and the chunk's list entries are
-        // spread evenly over all threads of the grid ----
+        // spread evenly over all threads of the grid; an edge to the previous
+        // step's vertex is recorded and left for later ----
         for (int c0 = 0; c0 < dout + din; c0 += kGreedyThreads) {
             const int j = c0 + tid;
             int beg = 0, len = 0, wv = 0;
@@ -227,6 +270,10 @@ __global__ void __launch_bounds__(kGreedyThreads, 1) k_greedy(GreedyArgs a) {
                 const bool out = j < dout;
                 const int t = c0 == 0 ? nt : out ? a.id1o[o0 + j] : a.id1i[i0 + j - dout];
                 const int w = c0 == 0 ? nwt : out ? a.w1o[o0 + j] : a.w1i[i0 + j - dout];
+                if (t == prev) {
+                    const int q = atomicAdd(&s_nfix, 1);
+                    if (q < kGreedyMaxFix) s_fix[q] = j;
+                }
                 const int f = map_s[t];
                 if (f >= 0 && w > 0) {
                     const int* off = out ? a.off2i : a.off2o;
@@ -272,12 +319,14 @@ __global__ void __launch_bounds__(kGreedyThreads, 1) k_greedy(GreedyArgs a) {
                 for (int u = 0; u < kGreedyUnroll; u++) {
                     if (k[u] < 0) continue;
                     const int c = min(wl[u] & 0x7fffffff, w2[u]);
-                    if (c > 0) atomicAdd(&a.acc[g2[u]], c);
+                    if (c > 0) atomicAdd(&acc[g2[u]], c);
                 }
             }
             __syncthreads();
         }
         const double4 r1 = a.ratio1[v1];
+        // one grid barrier per step: this step's scatter is complete and the
+        // previous step's slice bests are published
         if (!grid_barrier(a.bar)) return;
         if (step + 1 < a.n) {
             nv = a.order1[step + 1];
@@ -288,11 +337,37 @@ __global__ void __launch_bounds__(kGreedyThreads, 1) k_greedy(GreedyArgs a) {
                 nwt = tid < ndout ? a.w1o[no0 + tid] : a.w1i[ni0 + tid - ndout];
             }
         }
-        // ---- this CTA's best candidate (and acc cleared for the next step) ----
+        if (step > 0) {
+            greedy_decide(a, (step - 1) & 1, prev, map_s, taken, base, len, wbest);
+            // the edges of v1 to prev: their terms for this CTA's slice only
+            const int nfix = s_nfix;
+            const int f = map_s[prev];
+            if (nfix > 0 && f >= 0) {
+                const int nscan = nfix <= kGreedyMaxFix ? nfix : dout + din;
+                for (int q = 0; q < nscan; q++) {
+                    const int j = nfix <= kGreedyMaxFix ? s_fix[q] : q;
+                    const bool out = j < dout;
+                    const int t = out ? a.id1o[o0 + j] : a.id1i[i0 + j - dout];
+                    const int w = out ? a.w1o[o0 + j] : a.w1i[i0 + j - dout];
+                    if (t != prev || w <= 0) continue;
+                    const int* off = out ? a.off2i : a.off2o;
+                    const int* lid = out ? a.id2i : a.id2o;
+                    const int* lw = out ? a.w2i : a.w2o;
+                    for (int k = off[f] + tid; k < off[f + 1]; k += blockDim.x) {
+                        const int g = lid[k];
+                        if (g < base || g >= base + len) continue;
+                        const int c = min(w, lw[k]);
+                        if (c > 0) atomicAdd(&acc[g], c);
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        // ---- this CTA's best candidate (and its acc cleared for two steps on) ----
         GreedyBest best{-1.0 / 0.0, 0x7fffffff, -1};
         for (int l = tid; l < len; l += blockDim.x) {
-            const int al = __ldcg(&a.acc[base + l]);
-            if (al) a.acc[base + l] = 0;
+            const int al = __ldcg(&acc[base + l]);
+            if (al) acc[base + l] = 0;
             if (taken[l]) continue;
             const GreedyBest c{greedy_score(r1, r2_s[l], al), pos_s[l], base + l};
             if (better(c, best)) best = c;
@@ -313,33 +388,14 @@ __global__ void __launch_bounds__(kGreedyThreads, 1) k_greedy(GreedyArgs a) {
             __stcg(&dst->score, best.score);
             __stcg(&dst->pos, best.pos);
             __stcg(&dst->g, best.g);
-        }
-        if (!grid_barrier(a.bar)) return;
-        // ---- the grid's best, reduced by every CTA from the published bests ----
-        best = GreedyBest{-1.0 / 0.0, 0x7fffffff, -1};
-        for (int r = tid; r < (int)gridDim.x; r += blockDim.x) {
-            const GreedyBest* src = a.bests + par * gridDim.x + r;
-            const GreedyBest c{__ldcg(&src->score), __ldcg(&src->pos), __ldcg(&src->g)};
-            if (better(c, best)) best = c;
-        }
-        for (int o = 16; o; o >>= 1) {
-            GreedyBest y;
-            y.score = __shfl_xor_sync(0xffffffffu, best.score, o);
-            y.pos = __shfl_xor_sync(0xffffffffu, best.pos, o);
-            y.g = __shfl_xor_sync(0xffffffffu, best.g, o);
-            if (better(y, best)) best = y;
-        }
-        if (lane == 0) wbest[wid] = best;
-        __syncthreads();
-        if (tid == 0) {
-            for (int w = 1; w < kGreedyThreads / 32; w++)
-                if (better(wbest[w], best)) best = wbest[w];
-            map_s[v1] = best.g;
-            if (best.g >= base && best.g < base + len) taken[best.g - base] = 1;
-            if (blockIdx.x == 0) a.map[v1] = best.g;
+            s_nfix = 0;
         }
         __syncthreads();
+        prev = v1;
     }
+    // the last step's decision
+    if (!grid_barrier(a.bar)) return;
+    greedy_decide(a, (a.n - 1) & 1, prev, map_s, taken, a.n, 0, wbest);
 }
 
 struct HostLists {
@@ -526,8 +582,8 @@ extern "C" bm_status bm_greedy_match(int32_t n, int64_t e1, const int32_t* src1,
     unsigned* bar;
     GK(D.alloc(&feat1, n)); GK(D.alloc(&feat2, n)); GK(D.alloc(&ratio1, n)); GK(D.alloc(&ratio2, n));
     GK(D.alloc(&order1, n)); GK(D.alloc(&order2, n)); GK(D.alloc(&pos2, n)); GK(D.alloc(&mapd, n));
-    GK(D.alloc(&acc, n)); GK(D.alloc(&bests, 2 * (size_t)grid)); GK(D.alloc(&bar, 4));
-    GK(cudaMemsetAsync(acc, 0, (size_t)n * sizeof(int), st));
+    GK(D.alloc(&acc, 2 * (size_t)n)); GK(D.alloc(&bests, 2 * (size_t)grid)); GK(D.alloc(&bar, 4));
+    GK(cudaMemsetAsync(acc, 0, 2 * (size_t)n * sizeof(int), st));
     GK(cudaMemsetAsync(bar, 0, 4 * sizeof(unsigned), st));
     GreedyArgs A;
     A.n = n; A.slice = slice0;
