@@ -179,21 +179,11 @@ __device__ __forceinline__ void profit_row(const DevView<W16>& g, int a, int* ac
     const int n = g.n;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
     if (tid == 0) *s_nlong = 0;
-    if (is_hub) {  // the row starts from the tensor-core hub terms already in S
-        const int* row0 = g.S + (size_t)a * (size_t)n;
-        if ((n & 3) == 0) {
-            const int4* r4 = reinterpret_cast<const int4*>(row0);
-            int4* a4 = reinterpret_cast<int4*>(acc);
-            const int n4 = n >> 2;
-            int i = tid;
-            for (; i + 3 * (int)blockDim.x < n4; i += 4 * blockDim.x) {
-                const int4 x0 = r4[i], x1 = r4[i + blockDim.x], x2 = r4[i + 2 * blockDim.x], x3 = r4[i + 3 * blockDim.x];
-                a4[i] = x0; a4[i + blockDim.x] = x1; a4[i + 2 * blockDim.x] = x2; a4[i + 3 * blockDim.x] = x3;
-            }
-            for (; i < n4; i += blockDim.x) a4[i] = r4[i];
-        } else {
-            for (int i = tid; i < n; i += blockDim.x) acc[i] = row0[i];
-        }
+    // the row's scattered terms start from zero; with hubs, the tensor-core
+    // hub terms already in S are added when the row is written back
+    if ((n & 3) == 0) {
+        int4* a4 = reinterpret_cast<int4*>(acc);
+        for (int i = tid; i < (n >> 2); i += blockDim.x) a4[i] = make_int4(0, 0, 0, 0);
         if (tid == 0) acc[n] = 0;
     } else {
         for (int i = tid; i <= n; i += blockDim.x) acc[i] = 0;
@@ -290,9 +280,29 @@ __device__ __forceinline__ void profit_row(const DevView<W16>& g, int a, int* ac
     if ((n & 3) == 0) {
         int4* r4 = reinterpret_cast<int4*>(row);
         const int4* a4 = reinterpret_cast<const int4*>(acc);
-        for (int i = tid; i < (n >> 2); i += blockDim.x) r4[i] = a4[i];
+        if (is_hub) {
+            const int n4 = n >> 2;
+            int i = tid;
+            for (; i + 3 * (int)blockDim.x < n4; i += 4 * blockDim.x) {
+                int4 h[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) h[u] = r4[i + u * blockDim.x];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int4 v = a4[i + u * blockDim.x];
+                    r4[i + u * blockDim.x] = make_int4(h[u].x + v.x, h[u].y + v.y, h[u].z + v.z, h[u].w + v.w);
+                }
+            }
+            for (; i < n4; i += blockDim.x) {
+                const int4 h = r4[i], v = a4[i];
+                r4[i] = make_int4(h.x + v.x, h.y + v.y, h.z + v.z, h.w + v.w);
+            }
+        } else {
+            for (int i = tid; i < (n >> 2); i += blockDim.x) r4[i] = a4[i];
+        }
     } else {
-        for (int i = tid; i < n; i += blockDim.x) row[i] = acc[i];
+        if (is_hub) for (int i = tid; i < n; i += blockDim.x) row[i] += acc[i];
+        else for (int i = tid; i < n; i += blockDim.x) row[i] = acc[i];
     }
     __syncthreads();
 }
