@@ -216,8 +216,8 @@ def test_greedy_features_and_distance_match_reference(tmp_path):
         assert oracle.greedy_distance(f1, f2) == R.distance(f1, f2)
 
 
-@pytest.mark.parametrize("seed", [5, 6, 7])
-def test_greedy_match_structural_part_matches_reference(tmp_path, seed):
+@pytest.mark.parametrize("seed,n,e", [(5, 40, 160), (6, 40, 160), (7, 40, 160), (8, 150, 900)])
+def test_greedy_match_structural_part_matches_reference(tmp_path, seed, n, e):
     """With every G1 weight 0 the align term vanishes in both: the
     reference's own match_vertices then gives the oracle's matching.  (Equal
     totals keep index order in the reference because this C library's qsort
@@ -227,9 +227,8 @@ def test_greedy_match_structural_part_matches_reference(tmp_path, seed):
     except OSError:
         pytest.skip("reference not compiled on this machine")
     rng = np.random.default_rng(seed)
-    n = 40
-    s1, d1, w1 = _greedy_graph(rng, n, 160, zero_w=True)
-    s2, d2, w2 = _greedy_graph(rng, n, 160)
+    s1, d1, w1 = _greedy_graph(rng, n, e, zero_w=True)
+    s2, d2, w2 = _greedy_graph(rng, n, e)
     p1, p2 = str(tmp_path / "g1.csv"), str(tmp_path / "g2.csv")
     _write_csv(p1, s1, d1, w1)
     _write_csv(p2, s2, d2, w2)
