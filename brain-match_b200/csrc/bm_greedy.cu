@@ -398,25 +398,6 @@ __global__ void __launch_bounds__(kGreedyThreads, 1) k_greedy(GreedyArgs a) {
     greedy_decide(a, (a.n - 1) & 1, prev, map_s, taken, a.n, 0, wbest);
 }
 
-struct HostLists {
-    std::vector<int> off, id, w;
-};
-
-// CSR keyed by key[] (every entry, input order within a row).
-void host_csr(int n, long long m, const int* key, const int* other, const int* w, HostLists& L) {
-    L.off.assign((size_t)n + 1, 0);
-    for (long long i = 0; i < m; i++) L.off[key[i] + 1]++;
-    for (int v = 0; v < n; v++) L.off[v + 1] += L.off[v];
-    std::vector<int> pos(L.off.begin(), L.off.end() - 1);
-    L.id.resize(m);
-    L.w.resize(m);
-    for (long long i = 0; i < m; i++) {
-        const int p = pos[key[i]]++;
-        L.id[p] = other[i];
-        L.w[p] = w[i];
-    }
-}
-
 struct GreedyDev {
     std::vector<void*> bufs;
     ~GreedyDev() { for (void* p : bufs) cudaFree(p); }
@@ -441,38 +422,149 @@ struct GreedyDev {
         }                                                                             \
     } while (0)
 
-// Validates one graph's edges and converts ids to 0-based.  The message of a
+// Validates one graph's edges (ids in 1..n, weights >= 0).  The message of a
 // failure goes to err (the caller records it: this may run on a helper thread).
-bm_status load_edges(const char* fn, int n, long long m, const int32_t* s, const int32_t* d, const int32_t* w,
-                     std::vector<int>& s0, std::vector<int>& d0, std::vector<int>& w0, char* err, size_t cap) {
+bm_status check_edges(const char* fn, int n, long long m, const int32_t* s, const int32_t* d, const int32_t* w,
+                      char* err, size_t cap) {
     if (m < 0 || (m > 0 && (!s || !d || !w))) { snprintf(err, cap, "%s: bad edge arrays", fn); return BM_E_INPUT; }
-    s0.resize(m); d0.resize(m); w0.resize(m);
+    if (m > 0x7fffffffLL) { snprintf(err, cap, "%s: %lld edges (at most 2^31-1)", fn, m); return BM_E_INPUT; }
     for (long long i = 0; i < m; i++) {
         if (s[i] < 1 || s[i] > n || d[i] < 1 || d[i] > n) {
             snprintf(err, cap, "%s: edge %lld (%d,%d) outside 1..%d", fn, i, s[i], d[i], n);
             return BM_E_INPUT;
         }
         if (w[i] < 0) { snprintf(err, cap, "%s: edge %lld has negative weight %d", fn, i, w[i]); return BM_E_INPUT; }
-        s0[i] = s[i] - 1; d0[i] = d[i] - 1; w0[i] = w[i];
+    }
+    return BM_OK;
+}
+
+// ---- adjacency lists built on the device ----
+__global__ void k_to_zero_based(int* __restrict__ s, int* __restrict__ d, long long m) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (long long)gridDim.x * blockDim.x) {
+        s[i] -= 1;
+        d[i] -= 1;
+    }
+}
+__global__ void k_key_hist(const int* __restrict__ key, long long m, int* __restrict__ cnt) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (long long)gridDim.x * blockDim.x)
+        atomicAdd(&cnt[key[i] + 1], 1);
+}
+// Entry i goes to the next free slot of its row (order within a row: arrival).
+__global__ void k_csr_scatter(const int* __restrict__ key, const int* __restrict__ other, const int* __restrict__ w,
+                              long long m, int* __restrict__ cur, int* __restrict__ id, int* __restrict__ ww) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (long long)gridDim.x * blockDim.x) {
+        const int p = atomicAdd(&cur[key[i]], 1);
+        id[p] = other[i];
+        if (ww) ww[p] = w[i];
+    }
+}
+__global__ void k_pair_keys(const int* __restrict__ s, const int* __restrict__ d, long long m, int n,
+                            unsigned long long* __restrict__ key, int* __restrict__ idx) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (long long)gridDim.x * blockDim.x) {
+        key[i] = (unsigned long long)s[i] * (unsigned long long)n + (unsigned long long)d[i];
+        idx[i] = (int)i;
+    }
+}
+// 1 for the last entry of each run of equal (sorted) keys.
+__global__ void k_last_of_run(const unsigned long long* __restrict__ key, long long m, char* __restrict__ flag) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (long long)gridDim.x * blockDim.x)
+        flag[i] = (i + 1 == m || key[i] != key[i + 1]) ? 1 : 0;
+}
+__global__ void k_gather3(const int* __restrict__ sel, long long m, const int* __restrict__ s, const int* __restrict__ d,
+                          const int* __restrict__ w, int* __restrict__ s2, int* __restrict__ d2, int* __restrict__ w2) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (long long)gridDim.x * blockDim.x) {
+        const int j = sel[i];
+        s2[i] = s[j]; d2[i] = d[j]; w2[i] = w[j];
+    }
+}
+
+struct DevLists { int *off = nullptr, *id = nullptr, *w = nullptr; };
+
+// Lists keyed by key[] (0-based): off (n+1), id and, with w, weights.
+bm_status dev_csr(const char* fn, GreedyDev& D, int n, long long m, const int* key, const int* other, const int* w,
+                  DevLists& L, cudaStream_t st, int blocks) {
+    int *cnt, *cur;
+    GK(D.alloc(&L.off, (size_t)n + 1)); GK(D.alloc(&cnt, (size_t)n + 1)); GK(D.alloc(&cur, (size_t)n));
+    GK(D.alloc(&L.id, (size_t)m));
+    if (w) GK(D.alloc(&L.w, (size_t)m));
+    GK(cudaMemsetAsync(cnt, 0, ((size_t)n + 1) * sizeof(int), st));
+    if (m) k_key_hist<<<blocks, 256, 0, st>>>(key, m, cnt);
+    size_t tb = 0;
+    GK(cub::DeviceScan::InclusiveSum(nullptr, tb, cnt, L.off, n + 1, st));
+    char* tmp;
+    GK(D.alloc(&tmp, tb));
+    GK(cub::DeviceScan::InclusiveSum(tmp, tb, cnt, L.off, n + 1, st));
+    GK(cudaMemcpyAsync(cur, L.off, (size_t)n * sizeof(int), cudaMemcpyDeviceToDevice, st));
+    if (m) k_csr_scatter<<<blocks, 256, 0, st>>>(key, other, w, m, cur, L.id, w ? L.w : nullptr);
+    GK(cudaGetLastError());
+    return BM_OK;
+}
+
+// One entry per (src, dst) of a graph, the last weight given (a stable sort
+// keeps the input order among equal pairs): s, d, w of the kept entries.
+bm_status dev_dedup(const char* fn, GreedyDev& D, int n, long long m, const int* s, const int* d, const int* w,
+                    int** ks, int** kd, int** kw, long long* mk, cudaStream_t st, int blocks) {
+    unsigned long long *key, *key2;
+    int *idx, *perm, *sel, *nsel;
+    char* flag;
+    GK(D.alloc(&key, (size_t)m)); GK(D.alloc(&key2, (size_t)m)); GK(D.alloc(&idx, (size_t)m));
+    GK(D.alloc(&perm, (size_t)m)); GK(D.alloc(&sel, (size_t)m)); GK(D.alloc(&nsel, 1)); GK(D.alloc(&flag, (size_t)m));
+    int bits = 1;
+    while (bits < 64 && ((unsigned long long)n * (unsigned long long)n) >> bits) bits++;
+    if (m) {
+        k_pair_keys<<<blocks, 256, 0, st>>>(s, d, m, n, key, idx);
+        size_t tb = 0;
+        GK(cub::DeviceRadixSort::SortPairs(nullptr, tb, key, key2, idx, perm, (int)m, 0, bits, st));
+        char* tmp;
+        GK(D.alloc(&tmp, tb));
+        GK(cub::DeviceRadixSort::SortPairs(tmp, tb, key, key2, idx, perm, (int)m, 0, bits, st));
+        k_last_of_run<<<blocks, 256, 0, st>>>(key2, m, flag);
+        tb = 0;
+        GK(cub::DeviceSelect::Flagged(nullptr, tb, perm, flag, sel, nsel, (int)m, st));
+        char* tmp2;
+        GK(D.alloc(&tmp2, tb));
+        GK(cub::DeviceSelect::Flagged(tmp2, tb, perm, flag, sel, nsel, (int)m, st));
+        GK(cudaGetLastError());
+    } else {
+        GK(cudaMemsetAsync(nsel, 0, sizeof(int), st));
+    }
+    int h = 0;
+    GK(cudaMemcpyAsync(&h, nsel, sizeof(int), cudaMemcpyDeviceToHost, st));
+    GK(cudaStreamSynchronize(st));
+    *mk = h;
+    GK(D.alloc(ks, (size_t)h)); GK(D.alloc(kd, (size_t)h)); GK(D.alloc(kw, (size_t)h));
+    if (h) k_gather3<<<blocks, 256, 0, st>>>(sel, h, s, d, w, *ks, *kd, *kw);
+    GK(cudaGetLastError());
+    return BM_OK;
+}
+
+// The three raw edge arrays of a graph, 0-based, on the device.
+bm_status dev_edges(const char* fn, GreedyDev& D, long long m, const int32_t* s, const int32_t* d, const int32_t* w,
+                    int** ds, int** dd, int** dw, cudaStream_t st, int blocks) {
+    GK(D.alloc(ds, (size_t)m)); GK(D.alloc(dd, (size_t)m)); GK(D.alloc(dw, (size_t)m));
+    if (m) {
+        GK(cudaMemcpyAsync(*ds, s, (size_t)m * sizeof(int), cudaMemcpyHostToDevice, st));
+        GK(cudaMemcpyAsync(*dd, d, (size_t)m * sizeof(int), cudaMemcpyHostToDevice, st));
+        GK(cudaMemcpyAsync(*dw, w, (size_t)m * sizeof(int), cudaMemcpyHostToDevice, st));
+        k_to_zero_based<<<blocks, 256, 0, st>>>(*ds, *dd, m);
+        GK(cudaGetLastError());
     }
     return BM_OK;
 }
 
 // Features of one graph on the device: feat (int4), ratio (double4), and the
 // feature order (order[i] = vertex at place i).
-bm_status device_features(const char* fn, GreedyDev& D, int n, const HostLists& lo, const HostLists& li,
+bm_status device_features(const char* fn, GreedyDev& D, int n, const DevLists& lo, const DevLists& li,
                           int4* feat, double4* ratio, int* order, cudaStream_t st, int sms) {
-    int *offo, *ido, *offi, *idi, *r2, *c2, *val, *val2;
+    int *r2, *c2, *val, *val2;
     unsigned long long *key, *key2;
-    GK(D.up(&offo, lo.off)); GK(D.up(&ido, lo.id));
-    GK(D.up(&offi, li.off)); GK(D.up(&idi, li.id));
     GK(D.alloc(&r2, n)); GK(D.alloc(&c2, n));
     GK(D.alloc(&key, n)); GK(D.alloc(&key2, n)); GK(D.alloc(&val, n)); GK(D.alloc(&val2, n));
     const size_t bm = (size_t)((n + 31) / 32) * sizeof(unsigned);
     GK(cudaFuncSetAttribute(k_two_hop, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bm));
-    k_two_hop<<<sms * 4, 512, bm, st>>>(offo, ido, n, r2);
-    k_two_hop<<<sms * 4, 512, bm, st>>>(offi, idi, n, c2);
-    k_features<<<(n + 255) / 256, 256, 0, st>>>(offo, offi, r2, c2, n, feat, ratio, key, val);
+    k_two_hop<<<sms * 4, 512, bm, st>>>(lo.off, lo.id, n, r2);
+    k_two_hop<<<sms * 4, 512, bm, st>>>(li.off, li.id, n, c2);
+    k_features<<<(n + 255) / 256, 256, 0, st>>>(lo.off, li.off, r2, c2, n, feat, ratio, key, val);
     GK(cudaGetLastError());
     size_t tb = 0;
     GK(cub::DeviceRadixSort::SortPairs(nullptr, tb, key, key2, val, val2, n, 0, 64, st));
@@ -491,21 +583,24 @@ extern "C" bm_status bm_greedy_features(int32_t n, int64_t e, const int32_t* src
                                         const int32_t* w, int32_t* out) {
     const char* fn = "bm_greedy_features";
     if (n < 1 || !out) { set_err(nullptr, "%s: bad arguments", fn); return BM_E_INPUT; }
-    std::vector<int> s0, d0, w0;
     char err[256];
-    bm_status s = load_edges(fn, n, e, src, dst, w, s0, d0, w0, err, sizeof err);
-    if (s) set_err(nullptr, "%s", err);
-    if (s) return s;
-    HostLists lo, li;
-    host_csr(n, e, s0.data(), d0.data(), w0.data(), lo);
-    host_csr(n, e, d0.data(), s0.data(), w0.data(), li);
+    bm_status s = check_edges(fn, n, e, src, dst, w, err, sizeof err);
+    if (s) { set_err(nullptr, "%s", err); return s; }
     int dev = 0, sms = 0;
     GK(cudaGetDevice(&dev));
     GK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int blocks = sms * 8;
     GreedyDev D;
+    int *ds, *dd, *dw;
+    s = dev_edges(fn, D, e, src, dst, w, &ds, &dd, &dw, 0, blocks);
+    DevLists lo, li;
+    if (!s) s = dev_csr(fn, D, n, e, ds, dd, nullptr, lo, 0, blocks);
+    if (!s) s = dev_csr(fn, D, n, e, dd, ds, nullptr, li, 0, blocks);
     int4* feat; double4* ratio; int* order;
-    GK(D.alloc(&feat, n)); GK(D.alloc(&ratio, n)); GK(D.alloc(&order, n));
-    s = device_features(fn, D, n, lo, li, feat, ratio, order, 0, sms);
+    if (!s) {
+        GK(D.alloc(&feat, n)); GK(D.alloc(&ratio, n)); GK(D.alloc(&order, n));
+        s = device_features(fn, D, n, lo, li, feat, ratio, order, 0, sms);
+    }
     if (s) return s;
     GK(cudaMemcpy(out, feat, (size_t)n * sizeof(int4), cudaMemcpyDeviceToHost));
     return BM_OK;
@@ -516,43 +611,15 @@ extern "C" bm_status bm_greedy_match(int32_t n, int64_t e1, const int32_t* src1,
                                      const int32_t* w2, int32_t* map, bm_greedy_stats* stats) {
     const char* fn = "bm_greedy_match";
     if (n < 1 || !map) { set_err(nullptr, "%s: bad arguments", fn); return BM_E_INPUT; }
-    std::vector<int> s1, d1, ww1, s2, d2, ww2;
     bm_status s = BM_OK, s_2 = BM_OK;
     char err1[256], err2[256];
-    {
-        std::thread t([&] { s_2 = load_edges(fn, n, e2, src2, dst2, w2, s2, d2, ww2, err2, sizeof err2); });
-        s = load_edges(fn, n, e1, src1, dst1, w1, s1, d1, ww1, err1, sizeof err1);
+    {   // the two graphs are checked on two host threads
+        std::thread t([&] { s_2 = check_edges(fn, n, e2, src2, dst2, w2, err2, sizeof err2); });
+        s = check_edges(fn, n, e1, src1, dst1, w1, err1, sizeof err1);
         t.join();
     }
     if (s) { set_err(nullptr, "%s", err1); return s; }
     if (s_2) { set_err(nullptr, "%s", err2); return s_2; }
-    // the six host CSRs are independent but for G2's de-duplication, which
-    // reads G2's out-lists: built on host threads side by side
-    HostLists g1o, g1i, g2o, g2i, g2od, g2id;
-    std::vector<std::thread> th;
-    th.emplace_back([&] { host_csr(n, e1, s1.data(), d1.data(), ww1.data(), g1o); });
-    th.emplace_back([&] { host_csr(n, e1, d1.data(), s1.data(), ww1.data(), g1i); });
-    th.emplace_back([&] { host_csr(n, e2, d2.data(), s2.data(), ww2.data(), g2i); });
-    host_csr(n, e2, s2.data(), d2.data(), ww2.data(), g2o);
-    {   // G2 with one entry per (src, dst): the last weight given
-        std::vector<int> ks, kd, kw;
-        ks.reserve(e2); kd.reserve(e2); kw.reserve(e2);
-        std::vector<int> last((size_t)n, -1);
-        for (int u = 0; u < n; u++) {
-            // the last occurrence of each dst in u's row (rows keep input order)
-            for (int k = g2o.off[u + 1] - 1; k >= g2o.off[u]; k--) {
-                const int v = g2o.id[k];
-                if (last[v] == u) continue;
-                last[v] = u;
-                ks.push_back(u); kd.push_back(v); kw.push_back(g2o.w[k]);
-            }
-        }
-        const long long m = (long long)ks.size();
-        std::thread t2([&] { host_csr(n, m, kd.data(), ks.data(), kw.data(), g2id); });
-        host_csr(n, m, ks.data(), kd.data(), kw.data(), g2od);
-        t2.join();
-    }
-    for (auto& t : th) t.join();
     int dev = 0, sms = 0, optin = 0;
     GK(cudaGetDevice(&dev));
     GK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -587,12 +654,26 @@ extern "C" bm_status bm_greedy_match(int32_t n, int64_t e1, const int32_t* src1,
     GK(cudaMemsetAsync(bar, 0, 4 * sizeof(unsigned), st));
     GreedyArgs A;
     A.n = n; A.slice = slice0;
-    int* p;
-    GK(D.up(&p, g1o.off)); A.off1o = p; GK(D.up(&p, g1o.id)); A.id1o = p; GK(D.up(&p, g1o.w)); A.w1o = p;
-    GK(D.up(&p, g1i.off)); A.off1i = p; GK(D.up(&p, g1i.id)); A.id1i = p; GK(D.up(&p, g1i.w)); A.w1i = p;
-    GK(D.up(&p, g2od.off)); A.off2o = p; GK(D.up(&p, g2od.id)); A.id2o = p; GK(D.up(&p, g2od.w)); A.w2o = p;
-    GK(D.up(&p, g2id.off)); A.off2i = p; GK(D.up(&p, g2id.id)); A.id2i = p; GK(D.up(&p, g2id.w)); A.w2i = p;
-    GK(cudaEventRecord(ev[0], st));
+    const int blocks = sms * 8;
+    int *s1d, *d1d, *w1d, *s2d, *d2d, *w2d, *ks, *kd, *kw;
+    long long mk = 0;
+    DevLists g1o, g1i, g2o, g2i, g2od, g2id;
+    s = dev_edges(fn, D, e1, src1, dst1, w1, &s1d, &d1d, &w1d, st, blocks);
+    if (!s) s = dev_edges(fn, D, e2, src2, dst2, w2, &s2d, &d2d, &w2d, st, blocks);
+    if (s) return s;
+    GK(cudaEventRecord(ev[0], st));   // device time from here: lists, features, matching
+    if (!s) s = dev_csr(fn, D, n, e1, s1d, d1d, w1d, g1o, st, blocks);
+    if (!s) s = dev_csr(fn, D, n, e1, d1d, s1d, w1d, g1i, st, blocks);
+    if (!s) s = dev_csr(fn, D, n, e2, s2d, d2d, nullptr, g2o, st, blocks);
+    if (!s) s = dev_csr(fn, D, n, e2, d2d, s2d, nullptr, g2i, st, blocks);
+    if (!s) s = dev_dedup(fn, D, n, e2, s2d, d2d, w2d, &ks, &kd, &kw, &mk, st, blocks);
+    if (!s) s = dev_csr(fn, D, n, mk, ks, kd, kw, g2od, st, blocks);
+    if (!s) s = dev_csr(fn, D, n, mk, kd, ks, kw, g2id, st, blocks);
+    if (s) return s;
+    A.off1o = g1o.off; A.id1o = g1o.id; A.w1o = g1o.w;
+    A.off1i = g1i.off; A.id1i = g1i.id; A.w1i = g1i.w;
+    A.off2o = g2od.off; A.id2o = g2od.id; A.w2o = g2od.w;
+    A.off2i = g2id.off; A.id2i = g2id.id; A.w2i = g2id.w;
     s = device_features(fn, D, n, g1o, g1i, feat1, ratio1, order1, st, sms);
     if (!s) s = device_features(fn, D, n, g2o, g2i, feat2, ratio2, order2, st, sms);
     if (s) return s;

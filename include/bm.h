@@ -560,7 +560,8 @@ bm_status bm_learned_run(bm_ctx* ctx, bm_mlp* m, const bm_learned_opts* opts, in
  * vertices (the reference compares ids with indices).  Independent of any
  * bm_ctx; runs on the current device. */
 typedef struct {
-    float ms_features;   /* device time of both graphs' features and orders */
+    float ms_features;   /* device time of both graphs' adjacency lists,
+                            features and orders                            */
     float ms_match;      /* device time of the sequential matching          */
     int32_t reserved[2];
 } bm_greedy_stats;
