@@ -406,11 +406,6 @@ struct GreedyDev {
         if (e == cudaSuccess) bufs.push_back(*p);
         return e;
     }
-    template <class T> cudaError_t up(T** p, const std::vector<T>& h) {
-        cudaError_t e = alloc(p, h.size());
-        if (e == cudaSuccess && !h.empty()) e = cudaMemcpy(*p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
-        return e;
-    }
 };
 
 #define GK(call)                                                                      \
