@@ -43,6 +43,12 @@ CUB_KERNELS_PER_SWEEP = 16  # two radix sorts: histogram + exclusive sum + 6 one
 # learned sweep: contribution, dynamic features, column stats, normalise, pool, U/V, fused ranking,
 # score keys, gather, exact deltas, candidate keys, candidate extents, commit (plus two CUB radix sorts)
 OWN_KERNELS_PER_LEARNED_SWEEP = 13
+# greedy matching: 2 id conversions, 6 list builds (histogram + scatter), pair keys, last-of-run,
+# gather, 4 two-hop counts, 2 feature kernels, positions, the matching kernel (plus CUB sorts/scans)
+OWN_KERNELS_PER_GREEDY = 25
+# best swap: combine + per-row reduce, pick/commit, corner x2, column permutation, term update (scatter
+# and row paths), pS sync
+OWN_KERNELS_PER_LOOKUP_SWAP = 9
 
 
 def peaks():
@@ -509,6 +515,7 @@ def run_greedy(args, world, rank, local, pg):
                     "h2d_bytes_per_step": 4 * 3 * (len(g["src1"]) + len(g["src2"])),
                     "d2h_bytes_per_step": 4 * int(g["n"])},
             "greedy_score": greedy_score, "random_start_score": random_score,
+            "gpu_launches": args.steps * OWN_KERNELS_PER_GREEDY,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
         }
@@ -559,6 +566,7 @@ def run_lookup(args, world, rank, local, pg):
             "config": {"workload": "lookup_n18524", "n": int(g["n"]),
                        "step": "one exact best swap: pair combine over the table, pick, swap, table update"},
             "score_before": st["score_before"], "score_after": st["score_after"],
+            "gpu_launches": done * OWN_KERNELS_PER_LOOKUP_SWAP,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
         }
