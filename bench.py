@@ -274,6 +274,15 @@ def run_engine(args, g, world, rank, local, pg):
                       "frac": t_roof / t_meas,
                       "note": "above 1 because the sparse profit matrix skips the zero min terms "
                               "that the per-pair formula counts"}
+    # k_profit against the roof that binds it: one shared-memory atomic add per
+    # scattered min term, against the measured red.shared.add rate
+    profit_atomics = None
+    if red_peak and prof_ms > 0:
+        rate = terms / (prof_ms / 1e3)
+        profit_atomics = {"terms_per_launch": terms, "achieved_per_s": rate, "peak_per_s": red_peak,
+                          "frac": rate / red_peak,
+                          "note": "min terms scattered per launch / the launch's event time, against the "
+                                  "engine's shared-memory atomic microbenchmark"}
 
     # descent to convergence from the initial matching, device time: sweeps
     # that rebuild the profit matrix against sweeps that update it from the
@@ -327,6 +336,7 @@ def run_engine(args, g, world, rank, local, pg):
                          "kernel": "k_profit", "kernel_ms": prof_ms, "alg_bytes": alg_bytes,
                          "min_terms": terms},
             "sweep_roofline_int32": sweep_roof,
+            "profit_smem_atomics": profit_atomics,
             "descent": descent,
             "cpu_baseline": cpu,
             "gpu_launches": args.steps * (OWN_KERNELS_PER_SWEEP + CUB_KERNELS_PER_SWEEP),
