@@ -25,6 +25,11 @@
  *   orc_sweep / orc_triple_round / orc_quad_round  the best-per-row set commit that the engine
  *                      runs (candidates sorted by delta desc then ids, each
  *                      re-verified on the updated mapping).
+ *   orc_sweep_given / orc_triple_round_given  the same selection and commit
+ *                      from deltas the caller supplies (for sizes where the
+ *                      CPU cannot evaluate every pair or triple in a test;
+ *                      the caller checks those deltas by sampling)
+ *   orc_pair_deltas / orc_triple_deltas  many deltas at once, OpenMP
  * Graph semantics match the reference loaders: every G1 edge entry counts,
  * the last G2 weight for a (src,dst) pair wins, zero weights contribute 0.
  * Deviation, on purpose: a G1 self-loop (a,a,s) is scored exactly
@@ -114,7 +119,7 @@ void* orc_create(int n, long long e1, const int* s1, const int* d1, const int* w
     free(goff);
     g->g_off = off2; g->g_id = gi; g->g_w = gw;
     g->dense = NULL;
-    if (n <= 4096) {
+    if (n <= 8192) {
         g->dense = (int*)calloc((size_t)(n + 1) * (n + 1), sizeof(int));
         for (int v = 1; v <= n; v++)
             for (int i = off2[v]; i < off2[v + 1]; i++) g->dense[(size_t)v * (n + 1) + gi[i]] = gw[i];
@@ -206,6 +211,12 @@ void orc_all_deltas(void* p, const int* map, int* out) {
     }
 }
 
+/* deltas of k given pairs (m1[i], m2[i]) on one matching, OpenMP over pairs */
+void orc_pair_deltas(void* p, const int* map, long long k, const int* m1, const int* m2, int* out) {
+    #pragma omp parallel for schedule(dynamic, 256)
+    for (long long i = 0; i < k; i++) out[i] = orc_swap_delta(p, map, m1[i], m2[i]);
+}
+
 static void taint_nbrs(const orc* g, int x, unsigned char* taint) {
     for (int i = g->o_off[x]; i < g->o_off[x + 1]; i++) taint[g->o_id[i]] = 1;
     for (int i = g->i_off[x]; i < g->i_off[x + 1]; i++) taint[g->i_id[i]] = 1;
@@ -221,15 +232,18 @@ static int cmp_u64(const void* a, const void* b) {
  * verified, committed, best delta, deltas evaluated.  moves (optional, 3 ints
  * per commit: m1, m2, delta).
  */
-int orc_sweep(void* p, int* map, int max_candidates, int max_verify, long long* stats, int* moves) {
+/* The sweep's selection and commit given every pair's delta on the current
+ * matching (`all`, the linear pair order of orc_all_deltas).  orc_sweep
+ * computes `all` itself; orc_sweep_given takes it from the caller, so a test
+ * can run this rule on deltas it has checked row by row against the compiled
+ * reference where a full CPU evaluation would take minutes. */
+int orc_sweep_given(void* p, int* map, const int* all, int max_candidates, int max_verify,
+                    long long* stats, int* moves) {
     const orc* g = (const orc*)p;
     const int n = g->n;
     int* bestd = (int*)malloc(sizeof(int) * (n + 1));
     int* bestb = (int*)malloc(sizeof(int) * (n + 1));
     /* every unordered pair once; row a's best partner: largest delta, then smallest b */
-    long long np = (long long)n * (n - 1) / 2;
-    int* all = (int*)malloc(sizeof(int) * (size_t)(np ? np : 1));
-    orc_all_deltas(p, map, all);
     for (int a = 0; a <= n; a++) { bestd[a] = 0; bestb[a] = 0; }
     for (int a = 1; a <= n; a++) {
         long long base = (long long)(a - 1) * (2LL * n - a) / 2;
@@ -239,7 +253,6 @@ int orc_sweep(void* p, int* map, int max_candidates, int max_verify, long long* 
             if (bestb[b] == 0 || d > bestd[b] || (d == bestd[b] && a < bestb[b])) { bestd[b] = d; bestb[b] = a; }
         }
     }
-    free(all);
     uint64_t* keys = (uint64_t*)malloc(sizeof(uint64_t) * (n + 1));
     int nk = 0, best = 0;
     for (int a = 1; a <= n; a++) {
@@ -282,6 +295,17 @@ int orc_sweep(void* p, int* map, int max_candidates, int max_verify, long long* 
     }
     free(bestd); free(bestb); free(keys); free(used); free(taint);
     return committed;
+}
+
+int orc_sweep(void* p, int* map, int max_candidates, int max_verify, long long* stats, int* moves) {
+    const orc* g = (const orc*)p;
+    const int n = g->n;
+    long long np = (long long)n * (n - 1) / 2;
+    int* all = (int*)malloc(sizeof(int) * (size_t)(np ? np : 1));
+    orc_all_deltas(p, map, all);
+    int c = orc_sweep_given(p, map, all, max_candidates, max_verify, stats, moves);
+    free(all);
+    return c;
 }
 
 /* The reference's first-improvement order; returns commits, *passes = passes run. */
@@ -352,6 +376,14 @@ int orc_triple_delta(void* p, const int* map, int a, int b, int c, int rot) {
     return (int)(after - before);
 }
 
+/* both rotations of k given triples, out[2i + rot], OpenMP over triples */
+void orc_triple_deltas(void* p, const int* map, long long k, const int* a, const int* b, const int* c,
+                       int* out) {
+    #pragma omp parallel for schedule(dynamic, 64)
+    for (long long i = 0; i < k; i++)
+        for (int rot = 0; rot < 2; rot++) out[2 * i + rot] = orc_triple_delta(p, map, a[i], b[i], c[i], rot);
+}
+
 static uint64_t mix64(uint64_t x) {
     uint64_t z = x + 0x9E3779B97F4A7C15ULL;
     z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
@@ -381,8 +413,28 @@ int orc_sample_triple(void* p, uint64_t seed, int a, int j, int* b, int* c) {
 
 /* One 3-cycle round.  stats[0..6] = total delta, candidates, scanned, verified,
  * committed, best delta, valid triples. */
-int orc_triple_round(void* p, int* map, int partners, uint64_t seed, int max_candidates,
-                     int max_verify, long long* stats) {
+/* Every sampled triple of a round: b[(a-1)*partners + j], c[...] for slot j of
+ * vertex a, 0 where the slot has no valid triple.  Returns the valid count. */
+long long orc_triple_samples(void* p, uint64_t seed, int partners, int* bs, int* cs) {
+    const orc* g = (const orc*)p;
+    long long valid = 0;
+    for (int a = 1; a <= g->n; a++)
+        for (int j = 0; j < partners; j++) {
+            int b = 0, c = 0;
+            const size_t q = (size_t)(a - 1) * partners + j;
+            if (orc_sample_triple(p, seed, a, j, &b, &c)) { bs[q] = b; cs[q] = c; valid++; }
+            else { bs[q] = 0; cs[q] = 0; }
+        }
+    return valid;
+}
+
+/* One 3-cycle round; `given` (NULL: computed here) holds both rotations' deltas
+ * of every slot, given[2*((a-1)*partners + j) + rot], ignored for slots
+ * without a valid triple -- a test passes deltas it has checked by sampling
+ * against this file's triple delta, where evaluating all of them on the CPU
+ * would take minutes. */
+int orc_triple_round_given(void* p, int* map, int partners, uint64_t seed, const int* given,
+                           int max_candidates, int max_verify, long long* stats) {
     const orc* g = (const orc*)p;
     const int n = g->n;
     uint64_t* keys = (uint64_t*)malloc(sizeof(uint64_t) * (n + 1));
@@ -395,7 +447,8 @@ int orc_triple_round(void* p, int* map, int partners, uint64_t seed, int max_can
             if (!orc_sample_triple(p, seed, a, j, &b, &c)) continue;
             valid++;
             for (int rot = 0; rot < 2; rot++) {
-                int d = orc_triple_delta(p, map, a, b, c, rot);
+                int d = given ? given[2 * ((size_t)(a - 1) * partners + j) + rot]
+                              : orc_triple_delta(p, map, a, b, c, rot);
                 if (d > 0) {
                     uint64_t kk = ((uint64_t)(0x7fffffffu - (unsigned)d) << 32) |
                                   ((uint64_t)(a - 1) << 16) | ((unsigned)j << 1) | (unsigned)rot;
@@ -440,6 +493,11 @@ int orc_triple_round(void* p, int* map, int partners, uint64_t seed, int max_can
     }
     free(keys); free(used); free(taint);
     return committed;
+}
+
+int orc_triple_round(void* p, int* map, int partners, uint64_t seed, int max_candidates,
+                     int max_verify, long long* stats) {
+    return orc_triple_round_given(p, map, partners, seed, NULL, max_candidates, max_verify, stats);
 }
 
 /* ---- 4-set permutations ----

@@ -43,6 +43,14 @@ def orc_lib():
         L.orc_all_deltas.argtypes = [vp, vp, vp]
         L.orc_all_deltas.restype = None
         L.orc_sweep.argtypes = [vp, vp, i32, i32, vp, vp]
+        L.orc_sweep_given.argtypes = [vp, vp, vp, i32, i32, vp, vp]
+        L.orc_pair_deltas.argtypes = [vp, vp, i64, vp, vp, vp]
+        L.orc_pair_deltas.restype = None
+        L.orc_triple_deltas.argtypes = [vp, vp, i64, vp, vp, vp, vp]
+        L.orc_triple_deltas.restype = None
+        L.orc_triple_samples.restype = i64
+        L.orc_triple_samples.argtypes = [vp, u64, i32, vp, vp]
+        L.orc_triple_round_given.argtypes = [vp, vp, i32, u64, vp, i32, i32, vp]
         L.orc_first_improvement.restype = i64
         L.orc_first_improvement.argtypes = [vp, vp, i32, C.POINTER(i32), C.POINTER(i64)]
         L.orc_local_score.restype = i64
@@ -96,6 +104,23 @@ class Oracle:
         orc_lib().orc_all_deltas(self.h, _p(m), _p(out))
         return out
 
+    def pair_deltas(self, m, a, b):
+        """Deltas of the pairs (a[i], b[i]) on matching m."""
+        m = np.ascontiguousarray(m, np.int32)
+        a = np.ascontiguousarray(a, np.int32)
+        b = np.ascontiguousarray(b, np.int32)
+        out = np.zeros(len(a), np.int32)
+        orc_lib().orc_pair_deltas(self.h, _p(m), len(a), _p(a), _p(b), _p(out))
+        return out
+
+    def triple_deltas(self, m, a, b, c):
+        """Both rotations' deltas of the triples (a[i], b[i], c[i]), [k, 2]."""
+        m = np.ascontiguousarray(m, np.int32)
+        a, b, c = (np.ascontiguousarray(x, np.int32) for x in (a, b, c))
+        out = np.zeros(2 * len(a), np.int32)
+        orc_lib().orc_triple_deltas(self.h, _p(m), len(a), _p(a), _p(b), _p(c), _p(out))
+        return out.reshape(-1, 2)
+
     def sweep(self, m, max_candidates=0, max_verify=-1, want_moves=False):
         """Runs one sweep IN PLACE on m (int32 array); returns stats dict."""
         st = np.zeros(8, np.int64)
@@ -107,6 +132,37 @@ class Oracle:
         if want_moves:
             d["moves"] = mv[:3 * c].reshape(-1, 3)
         return d
+
+    def sweep_given(self, m, all_deltas, max_candidates=0, max_verify=-1):
+        """The sweep's selection and commit IN PLACE on m from supplied deltas
+        (the linear pair order of all_deltas); returns stats with the moves
+        as [k, 3] rows (lo, hi, delta) in commit order."""
+        d = np.ascontiguousarray(all_deltas, np.int32)
+        assert d.shape == (self.n * (self.n - 1) // 2,)
+        st = np.zeros(8, np.int64)
+        mv = np.zeros(3 * (self.n + 1), np.int32)
+        c = orc_lib().orc_sweep_given(self.h, _p(m), _p(d), max_candidates, max_verify, _p(st), _p(mv))
+        return dict(total_delta=int(st[0]), candidates=int(st[1]), scanned=int(st[2]), verified=int(st[3]),
+                    committed=int(st[4]), best_delta=int(st[5]), deltas=int(st[6]),
+                    moves=mv[:3 * c].reshape(-1, 3))
+
+    def triple_samples(self, seed, partners):
+        """(b, c) of every slot of a 3-cycle round, [n, partners] each, 0 where
+        the slot has no valid triple."""
+        b = np.zeros(self.n * partners, np.int32)
+        c = np.zeros(self.n * partners, np.int32)
+        orc_lib().orc_triple_samples(self.h, seed, partners, _p(b), _p(c))
+        return b.reshape(self.n, partners), c.reshape(self.n, partners)
+
+    def triple_round_given(self, m, partners, seed, deltas, max_candidates=0, max_verify=-1):
+        """A 3-cycle round IN PLACE on m from supplied deltas [n, partners, 2]."""
+        d = np.ascontiguousarray(deltas, np.int32)
+        assert d.shape == (self.n, partners, 2)
+        st = np.zeros(8, np.int64)
+        orc_lib().orc_triple_round_given(self.h, _p(m), partners, seed, _p(d), max_candidates, max_verify,
+                                         _p(st))
+        return dict(total_delta=int(st[0]), candidates=int(st[1]), scanned=int(st[2]), verified=int(st[3]),
+                    committed=int(st[4]), best_delta=int(st[5]), triples=int(st[6]))
 
     def best_swap_descent(self, m, max_swaps):
         """Best-swap descent IN PLACE on m; returns (pairs [k,2], deltas [k])."""

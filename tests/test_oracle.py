@@ -69,6 +69,45 @@ def test_oracle_sweep_rule_properties(cfg0):
         s = s2
 
 
+def test_oracle_rules_from_supplied_deltas_equal_the_full_rules(cfg0):
+    """orc_sweep_given / orc_triple_round_given (used where the CPU cannot
+    evaluate every pair or triple) make the same moves as the full rules when
+    given the oracle's own deltas; a planted delta changes the outcome, so the
+    supplied deltas are what decides.  The bulk delta functions equal the
+    one-at-a-time ones."""
+    g = cfg0
+    O = oracle.Oracle.from_pair(g)
+    m1, m2 = g["map0"].copy(), g["map0"].copy()
+    for caps in ((0, -1), (64, 5)):
+        d = O.all_deltas(m1)
+        a = O.sweep(m1, *caps, want_moves=True)
+        b = O.sweep_given(m2, d, *caps)
+        keys = ("total_delta", "candidates", "scanned", "verified", "committed")
+        assert {k: a[k] for k in keys} == {k: b[k] for k in keys}
+        assert np.array_equal(a["moves"], b["moves"]) and np.array_equal(m1, m2)
+    d = O.all_deltas(m1)
+    n = g["n"]
+    x, y = np.triu_indices(n, 1)
+    assert np.array_equal(O.pair_deltas(m1, x[:5000] + 1, y[:5000] + 1), d[:5000])
+    d[int(np.argmin(d))] = 10**9
+    assert O.sweep_given(m1.copy(), d)["best_delta"] == 10**9
+    # the 3-cycle round
+    P, seed = 16, 7
+    bs, cs = O.triple_samples(seed, P)
+    valid = bs > 0
+    a = np.repeat(np.arange(1, n + 1, dtype=np.int32), P).reshape(n, P)[valid]
+    td = O.triple_deltas(m1, a, bs[valid], cs[valid])
+    for i in range(0, len(a), 97):
+        for rot in range(2):
+            assert td[i, rot] == O.triple_delta(m1, int(a[i]), int(bs[valid][i]), int(cs[valid][i]), rot)
+    full = np.zeros((n, P, 2), np.int32)
+    full[valid] = td
+    r1, r2 = m1.copy(), m1.copy()
+    t1 = O.triple_round(r1, partners=P, seed=seed)
+    t2 = O.triple_round_given(r2, P, seed, full)
+    assert t1 == t2 and t1["triples"] == int(valid.sum()) and np.array_equal(r1, r2)
+
+
 def test_oracle_first_improvement_terminates():
     z = load_golden("small_n40")
     O = _pair(z)
