@@ -159,6 +159,38 @@ def cpu_reference(g, rows_target_s, seed=5, rows=None):
                 R=R, gm=gm, gf=gf, checksum=checksum)
 
 
+def cpu_racy(g, target_s, seed=6):
+    """The reference's racy OpenMP tool (src/graph-alignment-optimized-parallel.c:544-582,
+    compiled in place): its parallel loop over partners, with every improving
+    swap committed in a critical section followed by a full rescore, for one
+    seeded row against a bounded prefix of partners sized to ~target_s seconds,
+    from the random start.  Its deltas read a matching other threads change,
+    so its moves are not deterministic: it is timed as shipped, beside the
+    race-free row loop, and never used as a result."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    RQ = oracle.RefPar()
+    n = g["n"]
+    gm = RQ.graph(g["src1"], g["dst1"], g["w1"])
+    gf = RQ.graph(g["src2"], g["dst2"], g["w2"])
+    row = np.array([int(np.random.default_rng(seed).integers(1, n + 1))], np.int32)
+    k = min(n, 256)
+    t = time.perf_counter()
+    RQ.rows(gm, gf, g["map0"].copy(), row, k)
+    dt = max(time.perf_counter() - t, 1e-3)
+    k = int(min(n, max(k, k * target_s / dt)))
+    t = time.perf_counter()
+    cnt, commits, threads = RQ.rows(gm, gf, g["map0"].copy(), row, k)
+    dt = time.perf_counter() - t
+    RQ.free(gm)
+    RQ.free(gf)
+    return {"value": cnt / dt, "unit": "deltas/s", "cores": threads, "kind": "reference",
+            "sample": f"row {int(row[0])} x partners 1..{k} from the random start ({cnt} deltas, {commits} "
+                      f"commits with the tool's full rescore each, {dt:.1f} s)",
+            "note": "racy: deltas read a matching other threads change, and two commits in one row can "
+                    "give one image to two vertices; timed as shipped, not a result"}
+
+
 def run_reference(args, g, world, rank, pg):
     wl = args.workload
     if rank != 0:
@@ -318,6 +350,9 @@ def run_engine(args, g, world, rank, local, pg):
                 cpu = {"value": c["value"], "unit": "deltas/s", "cores": c["threads"], "kind": "reference",
                        "sample": f"{c['rows']} seeded rows x {n - 1} partners ({c['deltas']} deltas, "
                                  f"{c['seconds']:.1f} s), reference calculate_swap_delta under OpenMP"}
+                c["R"].free(c["gm"])
+                c["R"].free(c["gf"])
+                cpu["racy_tool"] = cpu_racy(g, 6.0)
             except OSError as e:
                 cpu = {"value": None, "unit": "deltas/s", "cores": 0, "kind": "reference", "sample": str(e)}
         line = {
@@ -384,6 +419,12 @@ def run_batch(args, world, rank, local, pg):
         maps = B.get_mappings()
     e2e_s = allreduce_max(pg, time.perf_counter() - t0)
     if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu:
+            try:
+                cpu = cpu_batch(pairs, args.cpu_seconds)
+            except OSError as e:
+                cpu = {"value": None, "unit": "deltas/s", "cores": 0, "kind": "reference", "sample": str(e)}
         h2d = sum(2 * (g["n"] + 1) * 4 for g in pairs)
         line = {
             "metric": "exact swap deltas/s (batched instances)", "value": value, "unit": "deltas/s",
@@ -396,6 +437,7 @@ def run_batch(args, world, rank, local, pg):
             "e2e": {"value": world * args.steps * info["total_pairs"] / e2e_s, "unit": "deltas/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d // 2},
             "committed_last_steps": int(commits.sum()),
+            "cpu_baseline": cpu,
             "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)
@@ -439,6 +481,12 @@ def run_triples(args, world, rank, local, pg):
     assert np.array_equal(E.get_mapping(), m_end)
     rot = sum(s["rotations"] for s in stats)
     if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu:
+            try:
+                cpu = cpu_triples(g, m_timed, 2000 + 0, args.cpu_seconds)
+            except OSError as e:
+                cpu = {"value": None, "unit": "rotations/s", "cores": 0, "kind": "reference", "sample": str(e)}
         line = {
             "metric": "exact 3-cycle rotation deltas/s", "value": world * rot / (ms / 1e3), "unit": "rotations/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
@@ -450,6 +498,149 @@ def run_triples(args, world, rank, local, pg):
                                     "round's moves (identical moves, asserted)"},
             "rounds": [{k: s[k] for k in ("triples", "committed", "verified", "score_after", "ms_sample",
                                          "ms_eval", "ms_commit", "ms_total")} for s in stats],
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    E.close()
+
+
+def cpu_triples(g, m, seed, target_s):
+    """The reference's 3-cycle delta: calculate_permutation_delta
+    (src/permutation.c:623-696, compiled in place) before and after each
+    rotation, under OpenMP over triples, on a seeded sample of the round's
+    triples (the same 256-partner two-hop sampling) sized to ~target_s seconds."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    O = oracle.Oracle.from_pair(g)
+    RP = oracle.RefPerm()
+    n = g["n"]
+    gm = RP.graph(g["src1"], g["dst1"], g["w1"])
+    gf = RP.graph(g["src2"], g["dst2"], g["w2"])
+    bs, cs = O.triple_samples(seed, 256)
+    valid = bs > 0
+    a = np.repeat(np.arange(1, n + 1, dtype=np.int32), 256).reshape(n, 256)[valid]
+    b, c = bs[valid], cs[valid]
+    rng = np.random.default_rng(seed)
+    k = 32
+    idx = rng.choice(len(a), k, replace=False)
+    t = time.perf_counter()
+    RP.triples_omp(gm, gf, m, a[idx], b[idx], c[idx])
+    dt = max(time.perf_counter() - t, 1e-3)
+    k = int(min(len(a), max(k, k * target_s / dt)))
+    idx = rng.choice(len(a), k, replace=False)
+    t = time.perf_counter()
+    _, threads = RP.triples_omp(gm, gf, m, a[idx], b[idx], c[idx])
+    dt = time.perf_counter() - t
+    RP.free(gm)
+    RP.free(gf)
+    return {"value": 2 * k / dt, "unit": "rotations/s", "cores": threads, "kind": "reference",
+            "sample": f"{k} seeded triples of the round ({2 * k} rotations, {dt:.1f} s), reference "
+                      "calculate_permutation_delta before/after each rotation under OpenMP"}
+
+
+def cpu_batch(pairs, target_s, seed=9):
+    """The reference's calculate_swap_delta (compiled in place, OpenMP over
+    partners as in src/alignment-omp.c:601-622) on seeded rows of four of the
+    batch's instances (smallest, largest, two between), each instance's
+    share of ~target_s seconds; deltas/s over all of them.  The reference
+    sizes every graph by NUM_NODES, so instances are built one at a time."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    R = oracle.RefGAO()
+    order = np.argsort([g["n"] for g in pairs])
+    pick = [order[0], order[len(order) // 3], order[2 * len(order) // 3], order[-1]]
+    rng = np.random.default_rng(seed)
+    tot_d, tot_s, threads, ns = 0, 0.0, 0, []
+    for i in pick:
+        g = pairs[int(i)]
+        n = int(g["n"])
+        gm = R.graph(g["src1"], g["dst1"], g["w1"])
+        gf = R.graph(g["src2"], g["dst2"], g["w2"])
+        t = time.perf_counter()
+        R.rows_omp(gm, gf, g["map0"], rng.choice(np.arange(1, n + 1), 2, replace=False).astype(np.int32), n)
+        per_row = max((time.perf_counter() - t) / 2, 1e-4)
+        rows = int(min(n, max(2, target_s / 4 / per_row)))
+        sample = rng.choice(np.arange(1, n + 1), rows, replace=False).astype(np.int32)
+        t = time.perf_counter()
+        cnt, _, threads = R.rows_omp(gm, gf, g["map0"], sample, n)
+        tot_s += time.perf_counter() - t
+        tot_d += cnt
+        ns.append((n, rows))
+        R.free(gm)
+        R.free(gf)
+    return {"value": tot_d / tot_s, "unit": "deltas/s", "cores": threads, "kind": "reference",
+            "sample": "seeded full rows of 4 instances (n, rows): " + ", ".join(f"({a}, {b})" for a, b in ns) +
+                      f"; {tot_d} deltas in {tot_s:.1f} s, reference calculate_swap_delta under OpenMP"}
+
+
+def run_first_improvement(args, world, rank, local, pg):
+    """The N=1,000 / 20,000-edge workload end to end: the reference's
+    sequential first-improvement order (src/graph-alignment-optimized.c:
+    515-577) from the random start until a pass commits nothing.  Engine:
+    bm_first_improvement; CPU: the reference's own loop compiled in place
+    (its commit validation and full rescore included).  Both make the same
+    moves; the final scores are asserted equal."""
+    import bm
+    import torch
+    torch.cuda.set_device(local)
+    p = dict(WORKLOADS["n1000_e20k"])
+    p["seed"] += rank
+    g = bm.generate(bm.gen_params(**p))
+    E = bm.Engine.from_pair(g)
+    for _ in range(args.warmup):
+        E.set_mapping(g["map0"])
+        E.first_improvement(10_000)
+    walls, devs = [], []
+    barrier(pg)
+    with Clocks(local) as clk:
+        for _ in range(args.steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            E.set_mapping(g["map0"])
+            E.timer_mark(0)
+            commits, passes = E.first_improvement(10_000)
+            E.timer_mark(1)
+            score = E.score()
+            m = E.get_mapping()
+            walls.append(time.perf_counter() - t0)
+            devs.append(E.timer_elapsed(0, 1) / 1e3)
+    barrier(pg)
+    dev = allreduce_max(pg, statistics.median(devs))
+    wall = allreduce_max(pg, statistics.median(walls))
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu:
+            try:
+                sys.path.insert(0, os.path.join(ROOT, "oracle"))
+                import oracle
+                R = oracle.RefGAO()
+                gm = R.graph(g["src1"], g["dst1"], g["w1"])
+                gf = R.graph(g["src2"], g["dst2"], g["w2"])
+                mr = g["map0"].copy()
+                t0 = time.perf_counter()
+                rscore, rcommits, rpasses = R.first_improvement(gm, gf, mr, g["n"], 10_000)
+                rs = time.perf_counter() - t0
+                R.free(gm)
+                R.free(gf)
+                assert rscore == score and np.array_equal(mr, m) and (rcommits, rpasses) == (commits, passes)
+                cpu = {"value": rs, "unit": "s", "cores": 1, "kind": "reference",
+                       "sample": f"the whole descent: {rcommits} commits over {rpasses} passes, final score "
+                                 f"{rscore} (identical matching to the engine's), m1, m2 over 1..n"}
+            except OSError as e:
+                cpu = {"value": None, "unit": "s", "cores": 0, "kind": "reference", "sample": str(e)}
+        line = {
+            "metric": "first-improvement descent time to the fixed point", "value": dev, "unit": "s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dev,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic",
+            "config": {"workload": "first_improvement_n1000", "n": int(g["n"]), "e1": int(len(g["src1"])),
+                       "step": "one sequential first-improvement descent from the random start to a pass "
+                               "without a commit"},
+            "final_score": score, "commits": commits, "passes": passes,
+            "e2e": {"value": wall, "unit": "s", "h2d_bytes_per_step": 4 * (int(g["n"]) + 1),
+                    "d2h_bytes_per_step": 4 * (int(g["n"]) + 1) + 8},
+            "cpu_baseline": cpu,
             "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)
@@ -761,7 +952,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--workload", default="n18524_e5m",
-                    choices=sorted(WORKLOADS) + ["batch64", "triples", "quads", "learned", "greedy", "lookup"])
+                    choices=sorted(WORKLOADS) + ["batch64", "triples", "quads", "learned", "greedy", "lookup",
+                                                 "first_improvement"])
     ap.add_argument("--train-sweeps", type=int, default=40)
     ap.add_argument("--graph", default="n18524_e5m", choices=sorted(WORKLOADS),
                     help="graph pair of the learned workload")
@@ -771,8 +963,8 @@ def main():
     ap.add_argument("--no-descent", action="store_true", help="skip the time-to-convergence descents")
     args = ap.parse_args()
     world, rank, local, pg = dist_setup()
-    import bm
-    if args.impl == "reference" and args.workload in ("batch64", "triples", "quads", "greedy", "lookup"):
+    if args.impl == "reference" and args.workload in ("batch64", "triples", "quads", "greedy", "lookup",
+                                                      "first_improvement"):
         if rank == 0:
             print(json.dumps({"impl": "reference", "unavailable": "the reference arm times the pairwise sweep "
                               "workloads; this workload's CPU baseline is the cpu_baseline of the engine line"}),
@@ -781,10 +973,10 @@ def main():
             pg.barrier()
             pg.destroy_process_group()
         return
-    if args.workload in ("batch64", "triples", "quads", "greedy", "lookup") or \
+    if args.workload in ("batch64", "triples", "quads", "greedy", "lookup", "first_improvement") or \
             (args.workload == "learned" and args.impl == "engine"):
         fn = {"batch64": run_batch, "triples": run_triples, "quads": run_quads, "learned": run_learned,
-              "greedy": run_greedy, "lookup": run_lookup}[args.workload]
+              "greedy": run_greedy, "lookup": run_lookup, "first_improvement": run_first_improvement}[args.workload]
         fn(args, world, rank, local, pg)
         if pg is not None:
             pg.barrier()
@@ -792,11 +984,15 @@ def main():
         return
     p = dict(WORKLOADS[args.graph if args.workload == "learned" else args.workload])
     p["seed"] += rank  # independent replica per rank
-    g = bm.generate(bm.gen_params(**p))
     if args.impl == "reference":
-        run_reference(args, g, world, rank, pg)
+        # the same seeded pair from the generator's host-only build, so the
+        # reference arm loads none of the engine's code
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        run_reference(args, oracle.generate(**p), world, rank, pg)
     else:
-        run_engine(args, g, world, rank, local, pg)
+        import bm
+        run_engine(args, bm.generate(bm.gen_params(**p)), world, rank, local, pg)
     if pg is not None:
         pg.barrier()
         pg.destroy_process_group()

@@ -1,10 +1,12 @@
 """ctypes binding of the CPU oracle -- TEST INFRASTRUCTURE ONLY.
 
-Loads oracle/_ref/liboracle.so (the C restatement, bm_oracle.c) and, when they
-were built, the reference's own code compiled in place:
-oracle/_ref/librefgao.so (src/graph-alignment-optimized.c),
-oracle/_ref/librefperm.so (src/permutation.c) and oracle/_ref/librefgreedy.so
-(src/greedy-feature-match.c).  Only tests/, smoke() and
+Loads oracle/_ref/liboracle.so (the C restatement, bm_oracle.c),
+oracle/_ref/libgen.so (the seeded workload generator, host C, so the CPU legs
+make their inputs without the engine library) and, when they were built, the
+reference's own code compiled in place: oracle/_ref/librefgao.so
+(src/graph-alignment-optimized.c), librefpar.so
+(src/graph-alignment-optimized-parallel.c), librefperm.so (src/permutation.c)
+and librefgreedy.so (src/greedy-feature-match.c).  Only tests/, smoke() and
 bench.py's CPU-baseline leg import this module, as the checker.
 """
 import ctypes as C
@@ -69,6 +71,47 @@ def orc_lib():
         L.orc_greedy_match.restype = None
         _orc = L
     return _orc
+
+
+class GenParams(C.Structure):
+    """bm_gen_params of include/bm.h."""
+    _fields_ = [("n", C.c_int32), ("wmax", C.c_int32), ("e", C.c_int64), ("seed", C.c_uint64),
+                ("alpha", C.c_double), ("geom_p", C.c_double), ("tail_prob", C.c_double),
+                ("tail_alpha", C.c_double), ("tail_scale", C.c_double), ("del_frac", C.c_double),
+                ("add_frac", C.c_double), ("jitter", C.c_int32), ("reserved", C.c_int32)]
+
+
+_gen = None
+
+
+def generate(n=1000, e=20000, seed=20261203, wmax=5000, tail_prob=0.0, **kw):
+    """The seeded graph pair of bm_generate (the same source, compiled into
+    oracle/_ref/libgen.so): dict of int32 arrays, 1-based ids."""
+    global _gen
+    if _gen is None:
+        L = C.CDLL(os.path.join(REF_DIR, "libgen.so"))
+        L.bm_gen_defaults.argtypes = [C.POINTER(GenParams)]
+        L.bm_gen_defaults.restype = None
+        L.bm_generate.argtypes = [C.POINTER(GenParams), vp, vp, vp, C.POINTER(i64), vp, vp, vp, vp, vp]
+        _gen = L
+    p = GenParams()
+    _gen.bm_gen_defaults(C.byref(p))
+    p.n, p.e, p.seed, p.wmax, p.tail_prob = n, e, seed, wmax, tail_prob
+    for k, v in kw.items():
+        setattr(p, k, v)
+    cap = e + int(np.ceil(p.add_frac * e)) + 1
+    s1, d1, w1 = (np.zeros(e, np.int32) for _ in range(3))
+    s2, d2, w2 = (np.zeros(cap, np.int32) for _ in range(3))
+    pi = np.zeros(n + 1, np.int32)
+    m0 = np.zeros(n + 1, np.int32)
+    e2 = i64()
+    st = _gen.bm_generate(C.byref(p), _p(s1), _p(d1), _p(w1), C.byref(e2), _p(s2), _p(d2), _p(w2), _p(pi),
+                          _p(m0))
+    if st != 0:
+        raise ValueError(f"bm_generate failed with status {st}")
+    k = e2.value
+    return dict(n=n, src1=s1, dst1=d1, w1=w1, src2=s2[:k].copy(), dst2=d2[:k].copy(), w2=w2[:k].copy(), pi=pi,
+                map0=m0)
 
 
 class Oracle:
@@ -303,6 +346,7 @@ class RefGAO:
         L.refgao_pair_deltas.restype = None
         L.refgao_rows_omp.restype = i64
         L.refgao_rows_omp.argtypes = [vp, vp, vp, vp, i32, i32, C.POINTER(i64), C.POINTER(i32)]
+        L.refgao_first_improvement.argtypes = [vp, vp, vp, i32, i32, C.POINTER(i64), C.POINTER(i32)]
         self.L = L
         self.NUM_NODES = L.refgao_num_nodes()
 
@@ -330,12 +374,62 @@ class RefGAO:
         self.L.refgao_pair_deltas(gm, gf, _p(mp), len(a), _p(a), _p(b), _p(out))
         return out
 
+    def first_improvement(self, gm, gf, m, n, max_passes):
+        """The reference's first-improvement loop on m (updated in place)
+        until a pass commits nothing; returns (score, commits, passes)."""
+        mp = self.pad(m)
+        c, p = i64(), i32()
+        s = self.L.refgao_first_improvement(gm, gf, _p(mp), int(n), int(max_passes), C.byref(c), C.byref(p))
+        m[:] = mp[:len(m)]
+        return s, c.value, p.value
+
+    def free(self, g):
+        self.L.refgao_graph_free(g)
+
     def rows_omp(self, gm, gf, m, rows, n):
         mp = self.pad(m)
         rows = np.ascontiguousarray(rows, np.int32)
         cs, nt = i64(), i32()
         cnt = self.L.refgao_rows_omp(gm, gf, _p(mp), _p(rows), len(rows), n, C.byref(cs), C.byref(nt))
         return cnt, cs.value, nt.value
+
+
+class RefPar:
+    """The reference's racy OpenMP tool, src/graph-alignment-optimized-parallel.c,
+    compiled in place: its parallel loop over partners driven for given rows."""
+
+    def __init__(self):
+        L = _load("librefpar.so")
+        if L is None:
+            raise OSError("oracle/_ref/librefpar.so not built")
+        L.refpar_graph_new.restype = vp
+        L.refpar_graph_add_many.argtypes = [vp, i64, vp, vp, vp]
+        L.refpar_graph_add_many.restype = None
+        L.refpar_graph_free.argtypes = [vp]
+        L.refpar_graph_free.restype = None
+        L.refpar_rows.restype = i64
+        L.refpar_rows.argtypes = [vp, vp, vp, vp, i32, i32, C.POINTER(i64), C.POINTER(i32)]
+        self.L = L
+        self.NUM_NODES = L.refpar_num_nodes()
+
+    def graph(self, s, d, w):
+        g = self.L.refpar_graph_new()
+        a = [np.ascontiguousarray(x, np.int32) for x in (s, d, w)]
+        self.L.refpar_graph_add_many(g, len(a[0]), _p(a[0]), _p(a[1]), _p(a[2]))
+        return g
+
+    def free(self, g):
+        self.L.refpar_graph_free(g)
+
+    def rows(self, gm, gf, m, rows, n):
+        """Runs the rows on m (updated in place); returns (deltas, commits, threads)."""
+        mp = np.zeros(max(self.NUM_NODES, len(m) - 1) + 1, np.int32)
+        mp[:len(m)] = m
+        rows = np.ascontiguousarray(rows, np.int32)
+        c, nt = i64(), i32()
+        cnt = self.L.refpar_rows(gm, gf, _p(mp), _p(rows), len(rows), int(n), C.byref(c), C.byref(nt))
+        m[:] = mp[:len(m)]
+        return cnt, c.value, nt.value
 
 
 class RefPerm:
@@ -350,6 +444,9 @@ class RefPerm:
         L.refperm_graph_add_many.restype = None
         L.refperm_local_score.argtypes = [vp, vp, vp, vp, i32]
         L.refperm_score.argtypes = [vp, vp, vp]
+        L.refperm_graph_free.argtypes = [vp]
+        L.refperm_graph_free.restype = None
+        L.refperm_triples_omp.argtypes = [vp, vp, vp, i64, vp, vp, vp, vp]
         self.L = L
 
     def graph(self, s, d, w):
@@ -357,6 +454,19 @@ class RefPerm:
         a = [np.ascontiguousarray(x, np.int32) for x in (s, d, w)]
         self.L.refperm_graph_add_many(g, len(a[0]), _p(a[0]), _p(a[1]), _p(a[2]))
         return g
+
+    def free(self, g):
+        self.L.refperm_graph_free(g)
+
+    def triples_omp(self, gm, gf, m, a, b, c):
+        """Both rotations' deltas of the triples by the reference's local score
+        under OpenMP, [k, 2]; returns (deltas, threads)."""
+        mp = np.zeros(max(18524, len(m) - 1) + 1, np.int32)
+        mp[:len(m)] = m
+        a, b, c = (np.ascontiguousarray(x, np.int32) for x in (a, b, c))
+        out = np.zeros(2 * len(a), np.int32)
+        nt = self.L.refperm_triples_omp(gm, gf, _p(mp), len(a), _p(a), _p(b), _p(c), _p(out))
+        return out.reshape(-1, 2), nt
 
     def local_score(self, gm, gf, m, vs):
         mp = np.zeros(max(18524, len(m) - 1) + 1, np.int32)

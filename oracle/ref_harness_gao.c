@@ -65,3 +65,44 @@ long long refgao_rows_omp(void* gm, void* gf, int* mapping, const int* rows, int
     if (threads) *threads = nt;
     return cnt;
 }
+
+/*
+ * The first-improvement loop of optimize_mapping (src/graph-alignment-
+ * optimized.c:515-577) with the reference's own calculate_swap_delta,
+ * validate_mapping_changes and post-commit calculate_alignment_score, over
+ * m1, m2 in 1..n (ids above n have no edges and no positive delta), stopped
+ * after a pass without a commit or after max_passes (the reference loops
+ * forever and saves files; neither is timed here).  Returns the final score.
+ */
+int refgao_first_improvement(void* gm, void* gf, int* mapping, int n, int max_passes,
+                             long long* commits, int* passes) {
+    int* old_mapping = (int*)malloc(sizeof(int) * (NUM_NODES + 1));
+    int score = calculate_alignment_score((Graph*)gm, (Graph*)gf, mapping);
+    long long c = 0;
+    int pass = 0;
+    for (; pass < max_passes; pass++) {
+        long long before = c;
+        for (int m1 = 1; m1 <= n; m1++) {
+            for (int m2 = 1; m2 <= n; m2++) {
+                if (m1 == m2) continue;
+                const int f1 = mapping[m1], f2 = mapping[m2];
+                const int delta = calculate_swap_delta((Graph*)gm, (Graph*)gf, mapping, m1, m2);
+                if (delta > 0) {
+                    memcpy(old_mapping, mapping, sizeof(int) * (NUM_NODES + 1));
+                    mapping[m1] = f2;
+                    mapping[m2] = f1;
+                    score += delta;
+                    c++;
+                    validate_mapping_changes(old_mapping, mapping, NUM_NODES, m1, m2);
+                    const int verify = calculate_alignment_score((Graph*)gm, (Graph*)gf, mapping);
+                    if (verify != score) score = verify;
+                }
+            }
+        }
+        if (c == before) { pass++; break; }
+    }
+    free(old_mapping);
+    if (commits) *commits = c;
+    if (passes) *passes = pass;
+    return score;
+}

@@ -210,16 +210,15 @@ def test_config2_triple_round_at_full_size(cfg1):
         except OSError:
             RP = None
         if RP is not None:
+            # the reference's local score deduplicates edges by a linear scan
+            # (quadratic in the set's degree), so it checks 300 of the triples
             gm = RP.graph(g["src1"], g["dst1"], g["w1"])
             gf = RP.graph(g["src2"], g["dst2"], g["w2"])
-            for i in sample[-300:]:
-                x, y, z = int(a[i]), int(b[i]), int(c[i])
-                before = RP.local_score(gm, gf, m, [x, y, z])
-                for rot in range(2):
-                    r = m.copy()
-                    fx, fy, fz = m[x], m[y], m[z]
-                    r[x], r[y], r[z] = (fy, fz, fx) if rot == 0 else (fz, fx, fy)
-                    assert RP.local_score(gm, gf, r, [x, y, z]) - before == td[i, rot]
+            few = sample[:300]
+            rd, _ = RP.triples_omp(gm, gf, m, a[few], b[few], c[few])
+            assert np.array_equal(rd, td[few])
+            RP.free(gm)
+            RP.free(gf)
         full = np.zeros((n, P, 2), np.int32)
         full[valid] = td
         ost = O.triple_round_given(m, P, seed, full)
