@@ -17,6 +17,7 @@ BM_OK, BM_E_INPUT, BM_E_CUDA, BM_E_OVERFLOW, BM_E_TIMEOUT, BM_E_NOMEM, BM_E_STAT
 BM_FLAG_FORCE_I32 = 1
 BM_FLAG_NO_HUB_GEMM = 2
 BM_STATIC_MAX_PAIRS = 65536
+BM_STALL_HUB_GEMM, BM_STALL_COMMIT, BM_STALL_COMBINE, BM_STALL_GREEDY, BM_STALL_MLP_GEMM = 1, 2, 3, 4, 5
 
 
 class GenParams(C.Structure):
@@ -137,6 +138,7 @@ def lib():
         L.bm_timer_mark.argtypes = [vp, i32]
         L.bm_timer_elapsed.argtypes = [vp, i32, i32, C.POINTER(C.c_float)]
         L.bm_measure_peaks.argtypes = [i32, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.bm_test_stall.argtypes = [i32]
         L.bm_batch_create.argtypes = [C.POINTER(vp), i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, u32]
         L.bm_batch_destroy.argtypes = [vp]
         L.bm_batch_destroy.restype = None
@@ -190,6 +192,11 @@ class BMError(RuntimeError):
 def _check(st, ctx=None):
     if st != BM_OK:
         raise BMError(st, (lib().bm_last_error(ctx) or b"").decode())
+
+
+def test_stall(site):
+    """bm_test_stall: the next launch at `site` makes one bounded wait run out."""
+    _check(lib().bm_test_stall(int(site)))
 
 
 # ---- generator -------------------------------------------------------------

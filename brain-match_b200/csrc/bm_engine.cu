@@ -12,6 +12,8 @@
 #include <algorithm>
 #include <utility>
 #include <mutex>
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 #include <cub/device/device_radix_sort.cuh>
 #include "bm.h"
@@ -19,12 +21,28 @@
 #include "bm_triples.cuh"
 #include "bm_quads.cuh"
 #include "bm_select.cuh"
+#include "bm_combine_tma.cuh"
 #include "bm_hub.cuh"
 #include "bm_incr.cuh"
 
 using namespace bm;
 
 static thread_local char g_create_err[512];
+
+// Test hook: the site set by bm_test_stall, taken (and cleared) by the next
+// launch at that site.
+static std::atomic<int> g_stall{0};
+
+int take_stall(int site) {
+    int want = site;
+    return g_stall.compare_exchange_strong(want, 0) ? 1 : 0;
+}
+
+extern "C" bm_status bm_test_stall(int32_t site) {
+    if (site < 0 || site > BM_STALL_MLP_GEMM) return BM_E_INPUT;
+    g_stall.store(site);
+    return BM_OK;
+}
 
 void set_err(bm_ctx* c, const char* fmt, ...) {
     char* dst = c ? c->err : g_create_err;
@@ -143,6 +161,7 @@ static void free_ctx(bm_ctx* c) {
     for (auto& e : c->uev) if (e) cudaEventDestroy(e);
     if (c->work_sum) cudaFree(c->work_sum);
     if (c->part) cudaFree(c->part);
+    if (c->diagS) cudaFree(c->diagS);
     for (void* b : {(void*)c->hubs, (void*)c->is_hub, (void*)c->hubA, (void*)c->hubB, (void*)c->hub_err})
         if (b) cudaFree(b);
     if (c->cinfo) cudaFree(c->cinfo);
@@ -525,7 +544,8 @@ bm_status stage_profit(bm_ctx* ctx) {
         CK(cudaGetLastError());
         CK(cudaFuncSetAttribute(k_hub_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem));
         dim3 grid(ctx->Npad / kGemmN, ctx->Mpad / kGemmM);
-        k_hub_gemm<<<grid, kGemmThreads, kGemmSmem, ctx->st>>>(ctx->hubA, ctx->hubB, K, n, ctx->S, ctx->hub_err);
+        k_hub_gemm<<<grid, kGemmThreads, kGemmSmem, ctx->st>>>(ctx->hubA, ctx->hubB, K, n, ctx->S, ctx->hub_err,
+                                                               take_stall(BM_STALL_HUB_GEMM));
         CK(cudaGetLastError());
     }
     const size_t smem = (size_t)(n + 1) * sizeof(int);
@@ -635,12 +655,59 @@ bm_status stage_refresh(bm_ctx* ctx, int* mode) {
 template bm_status stage_refresh<true>(bm_ctx*, int*);
 template bm_status stage_refresh<false>(bm_ctx*, int*);
 
+// The tensor map of S for the TMA-fed combine: rows of n int32, 64x64 boxes,
+// zero fill outside the matrix.  Needs the row stride (4n bytes) to be a
+// multiple of 16; returns false (the caller keeps k_combine64) otherwise.
+static bool combine_tma_setup(bm_ctx* ctx) {
+    const int n = ctx->n;
+    if ((n & 3) != 0 || n < kCmbT) return false;
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    });
+    if (!encode) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)n, (cuuint64_t)n};
+    const cuuint64_t strides[1] = {(cuuint64_t)n * sizeof(int)};
+    const cuuint32_t box[2] = {kCmbT, kCmbT};
+    const cuuint32_t estr[2] = {1, 1};
+    if (encode(&ctx->tmS, CU_TENSOR_MAP_DATA_TYPE_INT32, 2, ctx->S, dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
+    if (cudaFuncSetAttribute(k_combine_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, kCmbSmem) != cudaSuccess)
+        return false;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_combine_tma, kCmbThreads, kCmbSmem) != cudaSuccess ||
+        per_sm < 1)
+        return false;
+    if (dalloc(ctx, &ctx->diagS, (size_t)n * sizeof(int)) != cudaSuccess) return false;
+    ctx->cmb_grid = ctx->num_sms * per_sm;
+    return true;
+}
+
 bm_status stage_combine(bm_ctx* ctx, int* all_out) {
     const int n = ctx->n;
     const int t = (n + kTile - 1) / kTile;
     if (!ctx->part) CK(dalloc(ctx, &ctx->part, (size_t)t * n * sizeof(unsigned long long)));
-    dim3 grid(t, t);
-    k_combine64<<<grid, 256, 0, ctx->st>>>(ctx->S, n, ctx->part, all_out);
+    if (!ctx->cmb_ready) {
+        ctx->cmb_ready = true;
+        if (!combine_tma_setup(ctx)) ctx->cmb_grid = 0;
+    }
+    if (!all_out && ctx->cmb_grid > 0) {
+        k_diag<<<(n + 255) / 256, 256, 0, ctx->st>>>(ctx->S, n, ctx->diagS);
+        const long long pairs = (long long)t * (t + 1) / 2;
+        const int grid = (int)std::min<long long>(ctx->cmb_grid, pairs);
+        k_combine_tma<<<grid, kCmbThreads, kCmbSmem, ctx->st>>>(ctx->tmS, ctx->diagS, n, t, ctx->part,
+                                                                 ctx->hub_err, take_stall(BM_STALL_COMBINE));
+    } else {
+        dim3 grid(t, t);
+        k_combine64<<<grid, 256, 0, ctx->st>>>(ctx->S, n, ctx->part, all_out);
+    }
     CK(cudaGetLastError());
     k_best_reduce<<<(n + 255) / 256, 256, 0, ctx->st>>>(ctx->part, n, t, ctx->rowbest);
     CK(cudaGetLastError());
@@ -696,7 +763,7 @@ static bm_status stage_commit(bm_ctx* ctx, const bm_sweep_opts* o) {
         CK(cudaMemset(ctx->cgrid, 0, commit_grid_ints() * sizeof(int)));
     }
     CK(launch_commit_group<W16>(view<W16>(ctx), ctx->ckeys_sorted, lim, max_verify, ctx->cstats, ctx->cinfo, ctas,
-                                ctx->cgrid, smem, ctx->st));
+                                ctx->cgrid, smem, ctx->st, ctas > 1 ? take_stall(BM_STALL_COMMIT) : 0));
     return BM_OK;
 }
 
@@ -763,8 +830,17 @@ extern "C" bm_status bm_sweep(bm_ctx* ctx, const bm_sweep_opts* opts, bm_sweep_s
     if (ctx->cgrid)
         CK(cudaMemcpyAsync(&cerr, ctx->cgrid, sizeof cerr, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
-    if (herr) { set_err(ctx, "bm_sweep: tensor-core hub GEMM wait timed out"); return BM_E_TIMEOUT; }
-    if (cerr) { set_err(ctx, "bm_sweep: set commit grid barrier wait timed out"); return BM_E_TIMEOUT; }
+    if (herr || cerr) {
+        // the matching may be partly committed and S is not trusted: the
+        // caller sets a matching again before the next call
+        set_err(ctx, "bm_sweep: %s wait timed out",
+                (herr & (1 << kCmbErrBit)) ? "pair combine tile" : herr ? "tensor-core hub GEMM"
+                                                                        : "set commit cluster barrier");
+        if (herr) CK(cudaMemset(ctx->hub_err, 0, sizeof(int)));
+        ctx->mapped = false;
+        ctx->S_exact = false;
+        return BM_E_TIMEOUT;
+    }
     ctx->score = before + cs.total_delta;
     if (stats) {
         memset(stats, 0, sizeof *stats);
@@ -868,6 +944,17 @@ static bm_status lookup_descent_impl(bm_ctx* ctx, int max_swaps, bm_lookup_stats
     }
     CK(cudaEventRecord(ctx->ev[2], ctx->st));
     CK(cudaEventSynchronize(ctx->ev[2]));
+    {
+        int herr = 0;
+        CK(cudaMemcpy(&herr, ctx->hub_err, sizeof herr, cudaMemcpyDeviceToHost));
+        if (herr & (1 << kCmbErrBit)) {
+            set_err(ctx, "bm_lookup_descent: pair combine tile wait timed out");
+            CK(cudaMemset(ctx->hub_err, 0, sizeof(int)));
+            ctx->mapped = false;
+            ctx->S_exact = false;
+            return BM_E_TIMEOUT;
+        }
+    }
     ctx->score = before + acc[0];
     if (st) {
         memset(st, 0, sizeof *st);

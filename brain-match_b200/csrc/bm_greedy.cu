@@ -127,6 +127,7 @@ struct GreedyArgs {
     GreedyBest* bests;                                    // [2][gridDim.x] per-CTA bests
     unsigned* bar;                                        // [0] arrivals [1] generation [2] error
     int* map;                                             // out: G1 -> G2 (0-based)
+    int stall;                                            // test hook: CTA 0 skips the first arrival
 };
 
 // Score of candidate g for the G1 vertex with ratios r1: the reference's
@@ -148,22 +149,26 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
 
 // Grid-wide barrier of the co-resident CTAs.  Each wait is bounded: after
 // kGreedySpinLimit polls the CTA records the error word and every CTA leaves
-// at its next barrier.  Returns false once the error word is set.
-__device__ bool grid_barrier(unsigned* bar) {
+// at its next barrier.  Returns false once the error word is set.  With
+// `stall` (the bm_test_stall hook) CTA 0 does not arrive and every CTA polls
+// only a few thousand times, so the barrier never completes and every CTA
+// leaves at it.
+__device__ bool grid_barrier(unsigned* bar, bool stall = false) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
         __threadfence();
         const unsigned gen = ld_acquire_u32(&bar[1]);
-        if (atomicAdd(&bar[0], 1u) == gridDim.x - 1) {
+        const unsigned limit = stall ? (1u << 12) : kGreedySpinLimit;
+        if (!(stall && blockIdx.x == 0) && atomicAdd(&bar[0], 1u) == gridDim.x - 1) {
             atomicExch(&bar[0], 0u);
             __threadfence();
             atomicAdd(&bar[1], 1u);
         } else {
             unsigned it = 0;
             while (ld_acquire_u32(&bar[1]) == gen) {
-                if (ld_acquire_u32(&bar[2]) || ++it > kGreedySpinLimit) {
+                if (ld_acquire_u32(&bar[2]) || ++it > limit) {
                     atomicExch(&bar[2], 1u);
                     ok = 0;
                     break;
@@ -327,7 +332,7 @@ __global__ void __launch_bounds__(kGreedyThreads, 1) k_greedy(GreedyArgs a) {
         const double4 r1 = a.ratio1[v1];
         // one grid barrier per step: this step's scatter is complete and the
         // previous step's slice bests are published
-        if (!grid_barrier(a.bar)) return;
+        if (!grid_barrier(a.bar, a.stall && step == 0)) return;
         if (step + 1 < a.n) {
             nv = a.order1[step + 1];
             no0 = a.off1o[nv]; ndout = a.off1o[nv + 1] - no0;
@@ -677,6 +682,7 @@ extern "C" bm_status bm_greedy_match(int32_t n, int64_t e1, const int32_t* src1,
     GK(cudaEventRecord(ev[1], st));
     A.order1 = order1; A.pos2 = pos2; A.ratio1 = ratio1; A.ratio2 = ratio2;
     A.acc = acc; A.bests = bests; A.bar = bar; A.map = mapd;
+    A.stall = take_stall(BM_STALL_GREEDY);
     void* kargs[] = {&A};
     GK(cudaLaunchCooperativeKernel((const void*)k_greedy, dim3(grid), dim3(kGreedyThreads), kargs, smem, st));
     GK(cudaEventRecord(ev[2], st));

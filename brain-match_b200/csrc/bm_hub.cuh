@@ -59,12 +59,15 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
 }
 
 // Bounded wait; returns false (and records it) if the barrier never flips.
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity, int* err) {
-    for (int i = 0; i < (1 << 22); i++)
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity, int* err, int limit = 1 << 22) {
+    for (int i = 0; i < limit; i++)
         if (mbar_try_wait(bar, parity)) return true;
     atomicOr(err, 1);
     return false;
 }
+
+// Polls of a wait that the stall test hook (bm_test_stall) makes run out.
+constexpr int kStallPolls = 1 << 12;
 
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(dst), "l"(src) : "memory");
@@ -90,7 +93,7 @@ __device__ __forceinline__ void load_stage(uint32_t sA, uint32_t sB, const uint8
 // A: Mpad x K, B: Npad x K, both row-major u8 (K-major); K a multiple of 128.
 static __global__ void __launch_bounds__(kGemmThreads, 1)
 k_hub_gemm(const uint8_t* __restrict__ A, const uint8_t* __restrict__ B, int K, int n,
-           int* __restrict__ S, int* __restrict__ err) {
+           int* __restrict__ S, int* __restrict__ err, int stall) {
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;                    // 1024-aligned stages
@@ -161,6 +164,11 @@ k_hub_gemm(const uint8_t* __restrict__ A, const uint8_t* __restrict__ B, int K, 
     if (KC > 0) {
         const int last = KC - 1;
         ok = ok && mbar_wait_bounded(bars + 8 * (last % kGemmStages), (last / kGemmStages) & 1, err);
+        // test hook: with every MMA of the tile complete, tile (0,0) also waits
+        // for the barrier's next phase, which no commit ever completes
+        if (stall && blockIdx.x == 0 && blockIdx.y == 0)
+            ok = ok && mbar_wait_bounded(bars + 8 * (last % kGemmStages), ((last / kGemmStages) + 1) & 1, err,
+                                         kStallPolls);
     }
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");

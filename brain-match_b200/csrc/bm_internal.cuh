@@ -3,11 +3,16 @@
 #pragma once
 #include <cstdio>
 #include <cstdarg>
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include "bm.h"
 #include "bm_kernels.cuh"
 
 using namespace bm;
+
+// Test hook (bm_test_stall): 1 if the next launch at `site` is to make one of
+// its bounded waits run out, clearing the request.
+int take_stall(int site);
 
 struct bm_ctx {
     int n = 0;
@@ -63,6 +68,11 @@ struct bm_ctx {
     cudaEvent_t uev[8] = {};       // bm_timer_* slots
     unsigned long long* work_sum = nullptr;
     unsigned long long* part = nullptr;   // per-tile best partners (combine)
+    // TMA-fed combine (n % 4 == 0): tensor map over S, S's diagonal, grid size
+    alignas(64) CUtensorMap tmS;
+    bool cmb_ready = false;
+    int cmb_grid = 0;
+    int* diagS = nullptr;
     // tensor-core hub terms
     int nh = 0, hubK = 0, Mpad = 0, Npad = 0;
     bool hubA_built = false;

@@ -129,8 +129,11 @@ __global__ void k_row_work(DevView<W16> g, const unsigned char* __restrict__ is_
 // Inside a row, warps take the row's G1 edges round robin and scatter the
 // matching G2 list; lists longer than kLongList are queued and then scattered
 // by the whole CTA, so a few hub lists cannot hold the row's barrier.
+// The queue is small enough (1 KB) that three CTAs of 512 threads with an
+// N = 18,524 row each (74 KB) share one SM; a row that queues more scatters
+// the rest warp by warp.
 constexpr int kLongList = 2048;
-constexpr int kLongQueue = 512;
+constexpr int kLongQueue = 128;
 
 // Scatters min(w1, w2) over list[i0, i1) into acc, lanes striding by `step`.
 template <bool W16>

@@ -520,8 +520,8 @@ template <int BN>
 static bm_status gemm(bm_mlp* M, const __nv_bfloat16* A, const __nv_bfloat16* B, int m, int n, int k, float* C,
                       const float* bias, int relu, __nv_bfloat16* Cb) {
     MK(cudaFuncSetAttribute(k_gemm_bf16<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, gemm_bf16_smem<BN>()));
-    k_gemm_bf16<BN><<<dim3(n / BN, m / kGemmM), kGemmThreads, gemm_bf16_smem<BN>(), M->cs>>>(A, B, m, n, k, C, bias,
-                                                                                              relu, Cb, M->err_d);
+    k_gemm_bf16<BN><<<dim3(n / BN, m / kGemmM), kGemmThreads, gemm_bf16_smem<BN>(), M->cs>>>(
+        A, B, m, n, k, C, bias, relu, Cb, M->err_d, take_stall(BM_STALL_MLP_GEMM));
     MK(cudaGetLastError());
     return BM_OK;
 }
@@ -565,7 +565,12 @@ static bm_status check_err(bm_mlp* M) {
     int e = 0;
     MK(cudaMemcpyAsync(&e, M->err_d, sizeof e, cudaMemcpyDeviceToHost, M->cs));
     MK(cudaStreamSynchronize(M->cs));
-    if (e) { snprintf(M->err, sizeof M->err, "tensor-core GEMM wait timed out"); return BM_E_TIMEOUT; }
+    if (e) {
+        // the call's results are not trusted; the network object stays usable
+        snprintf(M->err, sizeof M->err, "tensor-core GEMM wait timed out");
+        MK(cudaMemset(M->err_d, 0, sizeof(int)));
+        return BM_E_TIMEOUT;
+    }
     return BM_OK;
 }
 

@@ -22,7 +22,7 @@ template <int BN>
 static __global__ void __launch_bounds__(kGemmThreads, 1)
 k_gemm_bf16(const __nv_bfloat16* __restrict__ A, const __nv_bfloat16* __restrict__ B, int M, int N, int K,
             float* __restrict__ C, const float* __restrict__ bias, int relu, __nv_bfloat16* __restrict__ Cb,
-            int* __restrict__ err) {
+            int* __restrict__ err, int stall) {
     constexpr int kStage = (kGemmM + BN) * kGemmKC;                   // bytes per stage
     constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) |  // f32 accum, bf16 x bf16
                                 ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(kGemmM >> 4) << 24);
@@ -105,6 +105,10 @@ k_gemm_bf16(const __nv_bfloat16* __restrict__ A, const __nv_bfloat16* __restrict
     if (KC > 0) {
         const int last = KC - 1;
         ok = ok && mbar_wait_bounded(bars + 8 * (last % kGemmStages), (last / kGemmStages) & 1, err);
+        // test hook (bm_test_stall): the barrier's next phase never completes
+        if (stall && blockIdx.x == 0 && blockIdx.y == 0)
+            ok = ok && mbar_wait_bounded(bars + 8 * (last % kGemmStages), ((last / kGemmStages) + 1) & 1, err,
+                                         kStallPolls);
     }
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");

@@ -157,6 +157,7 @@ __device__ __forceinline__ void atomicOr_u16(uint16_t* p, uint16_t v) {
 struct CommitGrid {
     int nct;          // CTAs of the cluster (1: a single CTA, no exchange)
     int* err;         // bit 1 set when a cluster wait runs out
+    int stall = 0;    // test hook (bm_test_stall): no CTA arrives in the first exchange
 };
 
 __device__ __forceinline__ uint32_t cluster_map(uint32_t local_addr, uint32_t rank) {
@@ -168,16 +169,26 @@ __device__ __forceinline__ uint32_t cluster_map(uint32_t local_addr, uint32_t ra
 // Arrive on the step mbarrier of every CTA of the cluster, then wait (bounded)
 // for this CTA's to complete the phase; false on timeout.  Thread 0 of each
 // CTA does the arrivals and the wait; the CTA syncs around it.
-__device__ __forceinline__ bool cluster_step_sync(uint32_t bar, uint32_t phase, int nct, int* err) {
+//
+// A CTA whose wait runs out stays resident for one more full wait window
+// before it reports the timeout (and the caller leaves): a peer whose own wait
+// completed just then still reads this CTA's partial sums and arrives on its
+// mbarrier at the next step, and both must reach a CTA that has not exited.
+// That peer then times out at the next step in turn, so every CTA stops
+// within two steps.  `stall` (the test hook) skips this CTA's arrivals and
+// shortens both windows: when every CTA stalls, every wait runs out at the
+// same step and no CTA touches another's shared memory afterwards.
+__device__ __forceinline__ bool cluster_step_sync(uint32_t bar, uint32_t phase, int nct, int* err, bool stall = false) {
     __shared__ int s_cok;
     __syncthreads();
-    if (threadIdx.x < (unsigned)nct) {  // thread r arrives on CTA r's mbarrier
+    if (!stall && threadIdx.x < (unsigned)nct) {  // thread r arrives on CTA r's mbarrier
         const uint32_t rb = cluster_map(bar, threadIdx.x);
         asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" :: "r"(rb) : "memory");
     }
     if (threadIdx.x == 0) {
+        const int limit = stall ? (1 << 12) : (1 << 22);
         int ok = 0;
-        for (int it = 0; it < (1 << 22); it++) {
+        for (int it = 0; it < limit; it++) {
             uint32_t done;
             asm volatile(
                 "{\n\t.reg .pred p;\n\t"
@@ -186,7 +197,17 @@ __device__ __forceinline__ bool cluster_step_sync(uint32_t bar, uint32_t phase, 
                 : "=r"(done) : "r"(bar), "r"(phase) : "memory");
             if (done) { ok = 1; break; }
         }
-        if (!ok) atomicOr(err, 2);
+        if (!ok) {
+            // the linger window: as many polls again, whatever they return
+            // (a poll suspends while the phase is open and returns at once
+            // after it completes, so this lasts at least milliseconds)
+            for (int it = 0; it < limit; it++)
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%0], %1;\n\t}"
+                    :: "r"(bar), "r"(phase) : "memory");
+            atomicOr(err, 2);
+        }
         s_cok = ok;
     }
     __syncthreads();
@@ -436,7 +457,10 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
                 s_cpart[buf][tid][2] = (int)s_imask[tid];
             }
             if (tid < cnt) { s_corr[tid] = 0; s_cnt[tid] = 0; s_imask[tid] = 0; }
-            if (!cluster_step_sync(cbar, (uint32_t)buf, nct, grid.err)) { aborted = true; break; }
+            if (!cluster_step_sync(cbar, (uint32_t)buf, nct, grid.err, grid.stall && gstep == 0)) {
+                aborted = true;
+                break;
+            }
             if (tid < nct * cnt) {  // thread (c, j): CTA c's partials of pair j (integer sums: any order)
                 const int c = tid / cnt, j = tid - c * cnt;
                 const uint32_t q = cluster_map((uint32_t)__cvta_generic_to_shared(&s_cpart[buf][j][0]), (uint32_t)c);
@@ -573,7 +597,7 @@ __host__ __device__ inline size_t commit_grid_ints() { return 4; }
 template <bool W16>
 __host__ inline cudaError_t launch_commit_group(const DevView<W16>& g, const unsigned long long* keys, int lim,
                                                int max_verify, CommitStats* st, const int4* cinfo, int ctas,
-                                               int* buf, size_t smem, cudaStream_t stream);
+                                               int* buf, size_t smem, cudaStream_t stream, int stall = 0);
 
 // Shared memory bytes of commit_group for n vertices.
 __host__ __device__ inline size_t commit_group_smem(int n) {
@@ -591,10 +615,10 @@ k_commit_group(DevView<W16> g, const unsigned long long* __restrict__ keys, int 
 template <bool W16>
 __host__ inline cudaError_t launch_commit_group(const DevView<W16>& g, const unsigned long long* keys, int lim,
                                                int max_verify, CommitStats* st, const int4* cinfo, int ctas,
-                                               int* buf, size_t smem, cudaStream_t stream) {
+                                               int* buf, size_t smem, cudaStream_t stream, int stall) {
     cudaError_t e = cudaFuncSetAttribute(k_commit_group<W16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    CommitGrid grid{1, buf};
+    CommitGrid grid{1, buf, stall};
     if (ctas <= 1) {
         k_commit_group<W16><<<1, 1024, smem, stream>>>(g, keys, lim, max_verify, st, cinfo, grid);
         return cudaGetLastError();

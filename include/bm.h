@@ -245,6 +245,26 @@ bm_status bm_timer_elapsed(bm_ctx* ctx, int32_t start_slot, int32_t end_slot, fl
  */
 bm_status bm_measure_peaks(int32_t n, double* red_per_s, double* minadd_per_s);
 
+/*
+ * Test hook for the timeout paths; no counterpart in the reference.
+ * Every wait a kernel makes on another part of the GPU (an mbarrier that the
+ * tensor cores or a copy complete, a cluster or grid barrier) is bounded:
+ * when it runs out the kernel records an error word, waits (bounded) for its
+ * own copies in flight, releases what it holds and returns, and the call
+ * reports BM_E_TIMEOUT with the site in bm_last_error.  bm_test_stall(site)
+ * makes the next launch at that site take one such wait that nothing
+ * completes (CTA 0 skips an arrival, or waits for a barrier phase nothing
+ * opens), with a short limit -- no fault, trap or endless loop.  One site at
+ * a time, process-wide; 0 clears it.  After BM_E_TIMEOUT a context's matching
+ * may be partly committed: set a matching again before the next call.
+ */
+#define BM_STALL_HUB_GEMM   1   /* bm_sweep: tensor-core hub GEMM          */
+#define BM_STALL_COMMIT     2   /* bm_sweep: set commit cluster exchange   */
+#define BM_STALL_COMBINE    3   /* bm_sweep: TMA-fed pair combine          */
+#define BM_STALL_GREEDY     4   /* bm_greedy_match: grid barrier           */
+#define BM_STALL_MLP_GEMM   5   /* bm_mlp_*: tensor-core GEMM              */
+bm_status bm_test_stall(int32_t site);
+
 /* ---- Exact swap-lookup table ----
  * The reference's best-swap tools keep an n x n table of swap deltas
  * (src/best-swap/create-score-lookup.c:289-296) and a heap of its positive
