@@ -1295,13 +1295,9 @@ static bm_status static_pairs_addr(bm_ctx* ctx, int** out) {
         return BM_E_INPUT;
     }
     std::lock_guard<std::mutex> lock(g_static_mu);
-    if (!g_static_addr[ctx->dev]) {
-        int cur = -1;
-        CK(cudaGetDevice(&cur));
-        if (cur != ctx->dev) CK(cudaSetDevice(ctx->dev));
+    if (!g_static_addr[ctx->dev]) {   // the caller made ctx->dev current
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_static_pairs);
-        if (cur != ctx->dev) CK(cudaSetDevice(cur));
         if (e != cudaSuccess) {
             set_err(ctx, "bm_pair_deltas_static: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
             return BM_E_CUDA;
@@ -1330,19 +1326,32 @@ extern "C" bm_status bm_pair_deltas_static(bm_ctx* ctx, int64_t k, const int32_t
             return BM_E_INPUT;
         }
     }
+    // the copies and the launch run with the context's device current, whatever
+    // device the caller has current; the caller's device is restored on return
+    int cur = -1;
+    CK(cudaGetDevice(&cur));
+    if (cur != ctx->dev) CK(cudaSetDevice(ctx->dev));
     int* base = nullptr;
     bm_status s = static_pairs_addr(ctx, &base);
-    if (s) return s;
-    int* da = base;
-    int* db = base + BM_STATIC_MAX_PAIRS;
-    int* dout = base + 2 * BM_STATIC_MAX_PAIRS;
-    CK(cudaMemcpyAsync(da, m1, k * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
-    CK(cudaMemcpyAsync(db, m2, k * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
-    const long long blocks = std::min<long long>((k + 7) / 8, (long long)ctx->num_sms * 16);
-    if (ctx->w16) k_pair_deltas_static<true><<<(int)blocks, 256, 0, ctx->st>>>(view<true>(ctx), da, db, k, dout);
-    else k_pair_deltas_static<false><<<(int)blocks, 256, 0, ctx->st>>>(view<false>(ctx), da, db, k, dout);
-    CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(out, dout, k * sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
-    CK(cudaStreamSynchronize(ctx->st));
-    return BM_OK;
+    if (!s) {
+        int* da = base;
+        int* db = base + BM_STATIC_MAX_PAIRS;
+        int* dout = base + 2 * BM_STATIC_MAX_PAIRS;
+        cudaError_t e = cudaMemcpyAsync(da, m1, k * sizeof(int), cudaMemcpyHostToDevice, ctx->st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(db, m2, k * sizeof(int), cudaMemcpyHostToDevice, ctx->st);
+        if (e == cudaSuccess) {
+            const long long blocks = std::min<long long>((k + 7) / 8, (long long)ctx->num_sms * 16);
+            if (ctx->w16) k_pair_deltas_static<true><<<(int)blocks, 256, 0, ctx->st>>>(view<true>(ctx), da, db, k, dout);
+            else k_pair_deltas_static<false><<<(int)blocks, 256, 0, ctx->st>>>(view<false>(ctx), da, db, k, dout);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaMemcpyAsync(out, dout, k * sizeof(int), cudaMemcpyDeviceToHost, ctx->st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->st);
+        if (e != cudaSuccess) {
+            set_err(ctx, "bm_pair_deltas_static: %s", cudaGetErrorString(e));
+            s = BM_E_CUDA;
+        }
+    }
+    if (cur != ctx->dev) cudaSetDevice(cur);
+    return s;
 }

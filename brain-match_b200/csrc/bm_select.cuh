@@ -131,13 +131,17 @@ static __global__ void k_best_reduce(const unsigned long long* __restrict__ part
 // pair does not stall the step), accumulating each pair's correction
 // from moved neighbours (a flag check per entry; W2 is read only for moved
 // neighbours) and noting which earlier pairs of the step it shares a vertex
-// with or is G1-adjacent to.  Thread 0 then decides the pairs in order; a pair
-// that touches an earlier pair of the step that committed or is still
-// undecided is carried, in order, into the next step and scanned again.  A
-// pair's delta depends only on p at its vertices and their G1 neighbours, so
-// every decision equals the one-at-a-time rule's.  With a re-verification
-// budget the step stops at the first carried pair, so the budget is spent in
-// the sequential order.
+// with or is G1-adjacent to.  For an entry whose neighbour belongs to an
+// earlier pair i of the step, the scan also adds the change that pair i's
+// swap would make to this pair's delta into cc[j][i] (each G1 edge has one
+// endpoint outside the pair, so these changes add up).  Warp 0 then decides
+// the pairs in order: a pair sharing a vertex with an earlier committed pair
+// is skipped, a pair next to a moved vertex (an earlier step's, or an earlier
+// committed pair of this step) is re-verified as its sweep delta plus those
+// changes, and it commits iff that is > 0.  A pair's delta depends only on p
+// at its vertices and their G1 neighbours, so every decision equals the
+// one-at-a-time rule's, re-verification budget included, and no pair is
+// scanned twice.
 constexpr int kCG = 16;                // pairs per step of the cluster commit (at most 16: marks are 16-bit)
 constexpr int kCGBatch = 8;            // pairs per step of a one-CTA commit (batched instances)
 
@@ -245,7 +249,8 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
     int gstep = 0;      // steps taken, the same in every CTA
     bool aborted = false;
     __shared__ __align__(8) unsigned long long s_cbar;   // the step mbarrier (nct arrivals per phase)
-    __shared__ int s_cpart[2][CG][3];                   // this CTA's partial sums, by step parity
+    __shared__ int s_cpart[2][CG][3 + CG];              // this CTA's partial sums, by step parity
+    __shared__ int s_cc[CG][CG];   // s_cc[j][i]: change of pair j's delta if earlier pair i commits
     const uint32_t cbar = (uint32_t)__cvta_generic_to_shared(&s_cbar);
     if (nct > 1) {
         if (tid == 0) {
@@ -257,16 +262,16 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
         asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
     }
     for (int i = tid; i < n; i += blockDim.x) { used[i] = 0; p16[i] = (uint16_t)g.p[i]; mark[i] = 0; }
+    for (int i = tid; i < CG * CG; i += blockDim.x) (&s_cc[0][0])[i] = 0;
     if (tid == 0) { s_n = 0; s_k = 0; s_scanned = 0; p16[n] = (uint16_t)n; }
     long long total = 0, entries = 0;
-    int verified = 0, committed = 0, steps = 0, carried = 0;
+    int verified = 0, committed = 0, steps = 0;
     int pf_base = -1;                  // warp 0: start of the window prefetched into s_pfkey, s_pfinf
     __shared__ unsigned long long s_pfkey[32];
     __shared__ int4 s_pfinf[32][2];
-    __shared__ int s_inf2[CG][8];     // carried rows in transit
     __syncthreads();
     for (;;) {
-        // ---- warp 0: append live candidates after the carried ones, then the
+        // ---- warp 0: the next live candidates, then the
         //      per-pair list extents and their prefix (lane j = pair j) ----
         if (wid == 0) {
             int cnt = s_n, k = s_k, scanned = s_scanned;
@@ -380,6 +385,8 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
                 const int tot = __shfl_sync(0xffffffffu, incl, cnt - 1);
                 if (lane == 0) { entries += tot; steps++; }
             }
+        } else {   // the other warps clear the step's conditional changes
+            for (int q = tid - 32; q < CG * CG; q += blockDim.x - 32) (&s_cc[0][0])[q] = 0;
         }
         __syncthreads();
         const int cnt = s_n;
@@ -427,7 +434,26 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
                     const unsigned im = mark[x] & ((1u << j) - 1u);  // earlier pairs with vertex x
                     if (im) atomicOr(&s_imask[j], im);
                     const int a = s_lo[j], b = s_hi[j];
-                    if (x == a || x == b || !used[x]) continue;
+                    if (x == a || x == b) continue;
+                    if (!used[x]) {
+                        // x is in earlier pair(s) i of the step: what each one's swap
+                        // (x taking its partner's image) would change in this delta
+                        for (unsigned rest = im; rest; rest &= rest - 1) {
+                            const int i = __ffs(rest) - 1;
+                            const int px = p16[s_lo[i] == x ? s_hi[i] : s_lo[i]], qx = p16[x];
+                            const int pa = p16[a], pb = p16[b], w = EN::w(en[u]);
+                            int c;
+                            if (kind[u] == 0 || kind[u] == 2)
+                                c = (imin(w, g.w2(pb, px)) - imin(w, g.w2(pa, px))) -
+                                    (imin(w, g.w2(pb, qx)) - imin(w, g.w2(pa, qx)));
+                            else
+                                c = (imin(w, g.w2t(px, pb)) - imin(w, g.w2t(px, pa))) -
+                                    (imin(w, g.w2t(qx, pb)) - imin(w, g.w2t(qx, pa)));
+                            if (kind[u] >= 2) c = -c;
+                            if (c) atomicAdd(&s_cc[j][i], c);
+                        }
+                        continue;
+                    }
                     mv[u] = true;
                     const int pa = p16[a], pb = p16[b], px = p16[x], qx = q16[x];
                     if (kind[u] == 0 || kind[u] == 2) {  // out-edges of the pair's vertex: W2 rows of the images
@@ -456,21 +482,29 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
                 s_cpart[buf][tid][0] = s_corr[tid]; s_cpart[buf][tid][1] = s_cnt[tid];
                 s_cpart[buf][tid][2] = (int)s_imask[tid];
             }
+            if (tid < cnt * CG) {
+                const int j = tid / CG, i = tid - j * CG;
+                s_cpart[buf][j][3 + i] = s_cc[j][i];
+            }
+            __syncthreads();
             if (tid < cnt) { s_corr[tid] = 0; s_cnt[tid] = 0; s_imask[tid] = 0; }
+            if (tid < cnt * CG) (&s_cc[0][0])[tid] = 0;
             if (!cluster_step_sync(cbar, (uint32_t)buf, nct, grid.err, grid.stall && gstep == 0)) {
                 aborted = true;
                 break;
             }
-            if (tid < nct * cnt) {  // thread (c, j): CTA c's partials of pair j (integer sums: any order)
-                const int c = tid / cnt, j = tid - c * cnt;
-                const uint32_t q = cluster_map((uint32_t)__cvta_generic_to_shared(&s_cpart[buf][j][0]), (uint32_t)c);
-                int v0, v1, v2;
-                asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v0) : "r"(q) : "memory");
-                asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v1) : "r"(q + 4) : "memory");
-                asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v2) : "r"(q + 8) : "memory");
-                if (v0) atomicAdd(&s_corr[j], v0);
-                if (v1) atomicOr(&s_cnt[j], v1);
-                if (v2) atomicOr(&s_imask[j], (unsigned)v2);
+            for (int t = tid; t < nct * cnt * (3 + CG); t += blockDim.x) {
+                // (c, j, k): field k of CTA c's partials of pair j (integer sums: any order)
+                const int c = t / (cnt * (3 + CG)), r = t - c * (cnt * (3 + CG));
+                const int j = r / (3 + CG), k = r - j * (3 + CG);
+                const uint32_t q = cluster_map((uint32_t)__cvta_generic_to_shared(&s_cpart[buf][j][k]), (uint32_t)c);
+                int v;
+                asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v) : "r"(q) : "memory");
+                if (!v) continue;
+                if (k == 0) atomicAdd(&s_corr[j], v);
+                else if (k == 1) atomicOr(&s_cnt[j], v);
+                else if (k == 2) atomicOr(&s_imask[j], (unsigned)v);
+                else atomicAdd(&s_cc[j][k - 3], v);
             }
             __syncthreads();
         }
@@ -481,35 +515,24 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
         if (tid < cnt) { mark[my_lo] = 0; mark[my_hi] = 0; }
         if (wid == 0) {
             const bool in = lane < cnt;
-            const unsigned share = in ? s_share[lane] : 0u, touch = in ? (s_imask[lane] | share) : 0u;
-            const int moved = in ? s_cnt[lane] : 0, corr = in ? s_corr[lane] : 0, d0 = in ? s_d0[lane] : 0;
+            const unsigned share = in ? s_share[lane] : 0u, adj = in ? s_imask[lane] : 0u;
+            const int moved = in ? s_cnt[lane] : 0, d0 = in ? s_d0[lane] : 0;
+            int corr = in ? s_corr[lane] : 0;   // grows by cc[lane][i] when earlier pair i commits
             const int a = in ? s_lo[lane] : 0, b = in ? s_hi[lane] : 0;
             const unsigned dead = s_dead;
-            unsigned cm = 0, pm = 0;
-            bool stop = false;
+            unsigned cm = 0;
 #pragma unroll
             for (int j = 0; j < CG; j++) {
                 const unsigned sh_j = __shfl_sync(0xffffffffu, share, j);
-                const unsigned to_j = __shfl_sync(0xffffffffu, touch, j);
+                const unsigned ad_j = __shfl_sync(0xffffffffu, adj, j);
                 const int mv_j = __shfl_sync(0xffffffffu, moved, j);
                 const int co_j = __shfl_sync(0xffffffffu, corr, j);
                 const int d0_j = __shfl_sync(0xffffffffu, d0, j);
                 if (j >= cnt) continue;
-                const bool is_dead = ((dead >> j) & 1u) || (sh_j & cm);  // a vertex already moved
-                bool carry = stop;
-                if (!carry) {
-                    if (is_dead) continue;  // decided: skip
-                    if (to_j & (cm | pm)) carry = true;
-                }
-                if (carry) {
-                    if (max_verify >= 0) stop = true;
-                    carried++;
-                    pm |= 1u << j;
-                    continue;
-                }
+                if (((dead >> j) & 1u) || (sh_j & cm)) continue;   // a vertex already moved: skip
                 int d = d0_j;
                 bool ok = true;
-                if (mv_j > 0) {
+                if (mv_j > 0 || (ad_j & cm)) {                   // next to a moved vertex: re-verify
                     if (max_verify >= 0 && verified >= max_verify) ok = false;
                     else { verified++; d += co_j; }
                 }
@@ -517,6 +540,7 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
                     cm |= 1u << j;
                     total += d;
                     committed++;
+                    if (lane > j && lane < cnt) corr += s_cc[lane][j];
                 }
             }
             __syncwarp();
@@ -530,16 +554,7 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
                 }
                 used[a] = 1; used[b] = 1;
             }
-            const bool carried_me = (pm >> lane) & 1u;  // carried pairs move to the front, in order
-            const int q = __popc(pm & ((1u << lane) - 1u));
-            if (carried_me)
-                for (int t = 0; t < 8; t++) s_inf2[q][t] = s_inf[lane][t];
-            __syncwarp();
-            if (carried_me) {
-                s_lo[q] = a; s_hi[q] = b; s_d0[q] = d0;
-                for (int t = 0; t < 8; t++) s_inf[q][t] = s_inf2[q][t];
-            }
-            if (lane == 0) s_n = __popc(pm);
+            if (lane == 0) s_n = 0;
         }
         __syncthreads();
     }
@@ -553,7 +568,7 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
         st->committed = committed;
         st->steps = steps;
         st->entries = entries;
-        st->carried = carried;
+        st->carried = 0;   // every pair is decided in the step that scans it
     }
 }
 

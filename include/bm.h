@@ -133,8 +133,13 @@ bm_status bm_pair_deltas(bm_ctx* ctx, int64_t k, const int32_t* m1, const int32_
  * Limits and sharing:
  *   - k > BM_STATIC_MAX_PAIRS is rejected with BM_E_INPUT; split the work.
  *   - The first call on a device looks up the array's device address
- *     (cudaGetSymbolAddress, with that device current) and keeps it; make
- *     that first call before capturing any CUDA stream.
+ *     (cudaGetSymbolAddress, with that device current) and keeps it for the
+ *     life of the process; make that first call before capturing any CUDA
+ *     stream.  Each call makes the context's device current for its copies
+ *     and launch and restores the caller's device before it returns.
+ *   - The kept address belongs to the device's primary context: after a
+ *     cudaDeviceReset the library (every bm_ctx included) must not be used
+ *     again in that process.
  *   - All calls in the process share the one array, which keeps the last
  *     call's contents.  Nothing in it has to start at zero: each call writes
  *     every result it copies back.  Calls that overlap on the GPU (two

@@ -40,6 +40,31 @@ def test_static_matches_allocating_entry_point_on_two_calls_in_a_row(cfg0):
         assert np.array_equal(E.pair_deltas_static(a, b), E.pair_deltas(a, b))
 
 
+def test_static_calls_allocate_nothing(cfg0):
+    """Neither the context's device memory nor the device's free memory moves
+    across static calls made before any allocating call; the allocating entry
+    point, called afterwards, still gives the same deltas."""
+    import torch
+    g = cfg0
+    n = g["n"]
+    rng = np.random.default_rng(7)
+    with bm.Engine.from_pair(g) as E:
+        E.set_mapping(g["map0"])
+        a, b = _pairs(rng, n, 20_000)
+        first = E.pair_deltas_static(a, b)          # looks the array's address up
+        torch.cuda.synchronize()
+        held = E.info()["device_bytes"]
+        free0 = torch.cuda.mem_get_info()[0]
+        outs = [E.pair_deltas_static(*_pairs(np.random.default_rng(s), n, bm.BM_STATIC_MAX_PAIRS))
+                for s in (1, 2)]
+        torch.cuda.synchronize()
+        assert E.info()["device_bytes"] == held
+        assert torch.cuda.mem_get_info()[0] == free0
+        assert np.array_equal(first, E.pair_deltas(a, b))
+        for s, o in zip((1, 2), outs):
+            assert np.array_equal(o, E.pair_deltas(*_pairs(np.random.default_rng(s), n, bm.BM_STATIC_MAX_PAIRS)))
+
+
 def test_static_rejects_more_pairs_than_the_fixed_array(cfg0):
     g = cfg0
     with bm.Engine.from_pair(g) as E:
