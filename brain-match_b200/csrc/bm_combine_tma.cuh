@@ -30,7 +30,8 @@ constexpr int kCmbT = 64;                                // tile edge
 constexpr int kCmbStages = 3;                            // tile pairs in flight per CTA
 constexpr int kCmbTileBytes = kCmbT * kCmbT * 4;         // 16 KB
 constexpr int kCmbStageBytes = 2 * kCmbTileBytes;        // S[I][J] and S[J][I]
-constexpr int kCmbThreads = 256;
+constexpr int kCmbThreads = 512;                         // 16 warps: 4 sub-blocks x 4 step ranges
+constexpr int kCmbSteps = 8;                             // diagonal steps per warp
 constexpr int kCmbSmem = kCmbStages * kCmbStageBytes + 128 + 64;   // + alignment + barriers
 constexpr int kCmbErrBit = 4;
 
@@ -91,9 +92,10 @@ k_combine_tma(const __grid_constant__ CUtensorMap tm, const int* __restrict__ di
     unsigned char* basep = cmb_raw + (base - raw);
     const uint32_t bars = base + kCmbStages * kCmbStageBytes;
     __shared__ int s_db[kCmbT];                             // S[b][b] of the tile's columns
-    __shared__ unsigned long long s_rk[4][kCmbT], s_ck[4][kCmbT];
+    __shared__ unsigned long long s_rk[8][kCmbT], s_ck[8][kCmbT];
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    const int hr = wid & 1, hc = (wid >> 1) & 1, kh = wid >> 2;
+    // warp: 32x32 sub-block (row half hr, column half hc), steps kq*8 .. kq*8+7
+    const int hr = wid & 1, hc = (wid >> 1) & 1, kq = wid >> 2;
     const long long npairs = (long long)tiles * (tiles + 1) / 2;
     const long long step = gridDim.x;
     const long long first = blockIdx.x;
@@ -136,22 +138,36 @@ k_combine_tma(const __grid_constant__ CUtensorMap tm, const int* __restrict__ di
         const int r = 32 * hr + lane, a = a0 + r;
         const int da = a < n ? __ldg(&diag[a]) : 0;
         const bool diagt = ti == tj;
-        int rd = INT_MIN, rb = INT_MAX;       // row a's best (delta, partner)
-        int cd = INT_MIN, ca = INT_MAX;       // column (32 hc + lane)'s best (delta, partner)
-#pragma unroll 4
-        for (int k = 16 * kh; k < 16 * kh + 16; k++) {
-            const int c = 32 * hc + ((lane + k) & 31), b = b0 + c;
-            int d = INT_MIN;
-            if (a < n && b < n && a != b) d = sA[r * kCmbT + c] + sB[c * kCmbT + r] - da - s_db[c];
-            if (d != INT_MIN && (d > rd || (d == rd && b < rb))) { rd = d; rb = b; }
-            // column 32 hc + lane was taken at this step by lane (lane - k) mod 32
-            const int src = (lane - k) & 31;
-            const int dc = __shfl_sync(0xffffffffu, d, src);
-            const int ac = a0 + 32 * hr + src;
-            if (dc != INT_MIN && (dc > cd || (dc == cd && ac < ca))) { cd = dc; ca = ac; }
+        // bests as packed keys (delta + 2^31) << 32 | ~partner: larger delta,
+        // then smaller partner; 0 = none
+        unsigned long long rk = 0, ck = 0;
+        if (!diagt && a0 + kCmbT <= n && b0 + kCmbT <= n) {   // full off-diagonal tile: no checks
+#pragma unroll
+            for (int q = 0; q < kCmbSteps; q++) {
+                const int k = kCmbSteps * kq + q;
+                const int c = 32 * hc + ((lane + k) & 31);
+                const int d = sA[r * kCmbT + c] + sB[c * kCmbT + r] - da - s_db[c];
+                rk = kmax(rk, pack_best(d, b0 + c));
+                // column 32 hc + lane was taken at this step by lane (lane - k) mod 32
+                const int src = (lane - k) & 31;
+                const int dc = __shfl_sync(0xffffffffu, d, src);
+                ck = kmax(ck, pack_best(dc, a0 + 32 * hr + src));
+            }
+        } else {
+            for (int q = 0; q < kCmbSteps; q++) {
+                const int k = kCmbSteps * kq + q;
+                const int c = 32 * hc + ((lane + k) & 31), b = b0 + c;
+                const bool v = a < n && b < n && a != b;
+                const int d = v ? sA[r * kCmbT + c] + sB[c * kCmbT + r] - da - s_db[c] : 0;
+                if (v) rk = kmax(rk, pack_best(d, b));
+                const int src = (lane - k) & 31;
+                const int dc = __shfl_sync(0xffffffffu, d, src);
+                const bool vc = __shfl_sync(0xffffffffu, v ? 1 : 0, src) != 0;
+                if (vc) ck = kmax(ck, pack_best(dc, a0 + 32 * hr + src));
+            }
         }
-        s_rk[2 * hc + kh][r] = rb == INT_MAX ? 0ull : pack_best(rd, rb);
-        s_ck[2 * hr + kh][32 * hc + lane] = ca == INT_MAX ? 0ull : pack_best(cd, ca);
+        s_rk[2 * kq + hc][r] = rk;
+        s_ck[2 * kq + hr][32 * hc + lane] = ck;
         __syncthreads();   // stage s is free again, the partials are complete
         if (tid == 0) {
             const long long q = p + kCmbStages * step;
@@ -163,12 +179,16 @@ k_combine_tma(const __grid_constant__ CUtensorMap tm, const int* __restrict__ di
         }
         if (tid < kCmbT) {
             const int x = a0 + tid;
-            if (x < n)
-                part[(size_t)tj * n + x] = kmax(kmax(s_rk[0][tid], s_rk[1][tid]), kmax(s_rk[2][tid], s_rk[3][tid]));
+            unsigned long long k = s_rk[0][tid];
+#pragma unroll
+            for (int w = 1; w < 8; w++) k = kmax(k, s_rk[w][tid]);
+            if (x < n) part[(size_t)tj * n + x] = k;
         } else if (tid < 2 * kCmbT && !diagt) {   // a diagonal tile's rows already cover both orders
             const int c = tid - kCmbT, x = b0 + c;
-            if (x < n)
-                part[(size_t)ti * n + x] = kmax(kmax(s_ck[0][c], s_ck[1][c]), kmax(s_ck[2][c], s_ck[3][c]));
+            unsigned long long k = s_ck[0][c];
+#pragma unroll
+            for (int w = 1; w < 8; w++) k = kmax(k, s_ck[w][c]);
+            if (x < n) part[(size_t)ti * n + x] = k;
         }
         // s_rk / s_ck and s_db are rewritten only after the next tile's wait,
         // which every thread reaches through a barrier
