@@ -132,7 +132,7 @@ __global__ void k_row_work(DevView<W16> g, const unsigned char* __restrict__ is_
 // The queue is small enough (1 KB) that three CTAs of 512 threads with an
 // N = 18,524 row each (74 KB) share one SM; a row that queues more scatters
 // the rest warp by warp.
-constexpr int kLongList = 2048;
+constexpr int kLongList = 4096;
 constexpr int kLongQueue = 128;
 
 // Scatters min(w1, w2) over list[i0, i1) into acc, lanes striding by `step`.
