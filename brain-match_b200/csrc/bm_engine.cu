@@ -23,11 +23,14 @@
 #include "bm_select.cuh"
 #include "bm_combine_tma.cuh"
 #include "bm_hub.cuh"
+#include "bm_hub_ws.cuh"
 #include "bm_incr.cuh"
 
 using namespace bm;
 
 static thread_local char g_create_err[512];
+
+static bool hub_ws_setup(bm_ctx* ctx);
 
 // Test hook: the site set by bm_test_stall, taken (and cleared) by the next
 // launch at that site.
@@ -337,7 +340,7 @@ extern "C" bm_status bm_create(bm_ctx** out, int32_t n, int64_t e1, const int32_
                     for (int v : hv) flag[v] = 1;
                     ctx->nh = nh;
                     ctx->hubK = nh * kHubT;
-                    ctx->Mpad = (n + kGemmM - 1) / kGemmM * kGemmM;
+                    ctx->Mpad = (n + 2 * kGemmM - 1) / (2 * kGemmM) * (2 * kGemmM);  // whole 256-row tiles
                     ctx->Npad = (n + kGemmN - 1) / kGemmN * kGemmN;
                     CK(dalloc(ctx, &ctx->hubs, nh * sizeof(int)));
                     CK(cudaMemcpy(ctx->hubs, hv.data(), nh * sizeof(int), cudaMemcpyHostToDevice));
@@ -540,12 +543,23 @@ bm_status stage_profit(bm_ctx* ctx) {
             ctx->hubA_built = true;
         }
         CK(cudaMemsetAsync(ctx->hubB, 0, (size_t)ctx->Npad * K, ctx->st));
-        k_hub_build_B<W16><<<ctx->nh, 256, 0, ctx->st>>>(g, ctx->hubs, ctx->nh, K, ctx->hubB);
+        k_hub_build_B<W16><<<dim3(ctx->nh, 8), 256, 0, ctx->st>>>(g, ctx->hubs, ctx->nh, K, ctx->hubB);
         CK(cudaGetLastError());
-        CK(cudaFuncSetAttribute(k_hub_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem));
-        dim3 grid(ctx->Npad / kGemmN, ctx->Mpad / kGemmM);
-        k_hub_gemm<<<grid, kGemmThreads, kGemmSmem, ctx->st>>>(ctx->hubA, ctx->hubB, K, n, ctx->S, ctx->hub_err,
-                                                               take_stall(BM_STALL_HUB_GEMM));
+        if (!ctx->hub_ws_ready) {
+            ctx->hub_ws_ready = true;
+            ctx->hub_ws = hub_ws_setup(ctx);
+        }
+        const int mt = ctx->Mpad / kGemmM, nt = ctx->Npad / kGemmN;
+        if (ctx->hub_ws) {
+            const int mw = ctx->Mpad / kWsM;
+            const int grid = std::min(ctx->num_sms, mw * nt);
+            k_hub_gemm_ws<<<grid, kWsThreads, kWsSmem, ctx->st>>>(ctx->tmHubA, ctx->tmHubB, K, n, mw, nt, ctx->S,
+                                                                 ctx->hub_err, take_stall(BM_STALL_HUB_GEMM));
+        } else {
+            CK(cudaFuncSetAttribute(k_hub_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem));
+            k_hub_gemm<<<dim3(nt, mt), kGemmThreads, kGemmSmem, ctx->st>>>(ctx->hubA, ctx->hubB, K, n, ctx->S,
+                                                                         ctx->hub_err, take_stall(BM_STALL_HUB_GEMM));
+        }
         CK(cudaGetLastError());
     }
     const size_t smem = (size_t)(n + 1) * sizeof(int);
@@ -658,9 +672,7 @@ template bm_status stage_refresh<false>(bm_ctx*, int*);
 // The tensor map of S for the TMA-fed combine: rows of n int32, 64x64 boxes,
 // zero fill outside the matrix.  Needs the row stride (4n bytes) to be a
 // multiple of 16; returns false (the caller keeps k_combine64) otherwise.
-static bool combine_tma_setup(bm_ctx* ctx) {
-    const int n = ctx->n;
-    if ((n & 3) != 0 || n < kCmbT) return false;
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
     static std::once_flag once;
     std::call_once(once, [] {
@@ -670,6 +682,41 @@ static bool combine_tma_setup(bm_ctx* ctx) {
             q == cudaDriverEntryPointSuccess)
             encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
     });
+    return encode;
+}
+
+// Tensor maps of the hub GEMM's u8 operands (rows of K bytes; boxes of one
+// 128-byte K-chunk of 256 A rows or 256 B rows, 128-byte swizzle) for the
+// persistent warp-specialised kernel; false keeps the one-tile-per-CTA kernel.
+static bool hub_ws_setup(bm_ctx* ctx) {
+    PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+    if (!encode || ctx->hubK % kGemmKC != 0) return false;
+    const cuuint32_t estr[2] = {1, 1};
+    const cuuint64_t dA[2] = {(cuuint64_t)ctx->hubK, (cuuint64_t)ctx->Mpad};
+    const cuuint64_t dB[2] = {(cuuint64_t)ctx->hubK, (cuuint64_t)ctx->Npad};
+    const cuuint64_t st[1] = {(cuuint64_t)ctx->hubK};
+    const cuuint32_t bA[2] = {kGemmKC, kWsM}, bB[2] = {kGemmKC, kGemmN};
+    if (encode(&ctx->tmHubA, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, ctx->hubA, dA, st, bA, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
+    if (encode(&ctx->tmHubB, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, ctx->hubB, dB, st, bB, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
+    if (cudaFuncSetAttribute(k_hub_gemm_ws, cudaFuncAttributeMaxDynamicSharedMemorySize, kWsSmem) != cudaSuccess)
+        return false;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_hub_gemm_ws, kWsThreads, kWsSmem) != cudaSuccess ||
+        per_sm != 1)
+        return false;
+    return true;
+}
+
+static bool combine_tma_setup(bm_ctx* ctx) {
+    const int n = ctx->n;
+    if ((n & 3) != 0 || n < kCmbT) return false;
+    PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
     if (!encode) return false;
     const cuuint64_t dims[2] = {(cuuint64_t)n, (cuuint64_t)n};
     const cuuint64_t strides[1] = {(cuuint64_t)n * sizeof(int)};

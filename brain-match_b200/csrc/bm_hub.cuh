@@ -237,15 +237,20 @@ template <bool W16>
 __global__ void k_hub_build_B(DevView<W16> g, const int* __restrict__ hubs, int nh, int K,
                               uint8_t* __restrict__ B) {
     typedef Ent<W16> EN;
+    // hub h's list is split over gridDim.y blocks; a row's kHubT = 8 threshold
+    // bytes go out as one 8-byte store
+    static_assert(kHubT == 8, "one 64-bit store per entry");
     for (int h = blockIdx.x; h < nh; h += gridDim.x) {
         const int f = g.p[hubs[h]];
         const int s0 = g.off2o[f], s1 = g.off2o[f + 1];  // f == n (unmatched): empty
-        for (int i = s0 + threadIdx.x; i < s1; i += blockDim.x) {
+        for (int i = s0 + blockIdx.y * blockDim.x + threadIdx.x; i < s1; i += gridDim.y * blockDim.x) {
             const typename EN::T e = g.ent2oP[i];
             const int b = EN::id(e), w = EN::w(e);
             if (b >= g.n) continue;  // image without a preimage
-            uint8_t* row = B + (size_t)b * K + h * kHubT;
-            for (int t = 0; t < kHubT; t++) row[t] = (uint8_t)(w >= t + 1);
+            unsigned long long v = 0;
+#pragma unroll
+            for (int t = 0; t < kHubT; t++) v |= (unsigned long long)(w >= t + 1) << (8 * t);
+            *reinterpret_cast<unsigned long long*>(B + (size_t)b * K + h * kHubT) = v;
         }
     }
 }

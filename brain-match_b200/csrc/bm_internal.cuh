@@ -70,6 +70,10 @@ struct bm_ctx {
     unsigned long long* part = nullptr;   // per-tile best partners (combine)
     // TMA-fed combine (n % 4 == 0): tensor map over S, S's diagonal, grid size
     alignas(64) CUtensorMap tmS;
+    // persistent warp-specialised hub GEMM: tensor maps of its operands
+    alignas(64) CUtensorMap tmHubA;
+    alignas(64) CUtensorMap tmHubB;
+    bool hub_ws_ready = false, hub_ws = false;
     bool cmb_ready = false;
     int cmb_grid = 0;
     int* diagS = nullptr;
