@@ -142,7 +142,8 @@ static __global__ void k_best_reduce(const unsigned long long* __restrict__ part
 // at its vertices and their G1 neighbours, so every decision equals the
 // one-at-a-time rule's, re-verification budget included, and no pair is
 // scanned twice.
-constexpr int kCG = 16;                // pairs per step of the cluster commit (at most 16: marks are 16-bit)
+constexpr int kCG = 16;                // pairs per step of the cluster commit (16-bit vertex marks)
+constexpr int kCGWide = 32;            // ... when 32-bit marks fit in shared memory
 constexpr int kCGBatch = 8;            // pairs per step of a one-CTA commit (batched instances)
 
 // 16-bit atomic OR in shared memory through the aligned 32-bit word.
@@ -220,6 +221,10 @@ __device__ __forceinline__ bool cluster_step_sync(uint32_t bar, uint32_t phase, 
 
 // The set commit of one instance; all 1024 threads of the block call it.
 // smem: commit_group_smem(n) bytes of dynamic shared memory.
+// Per-vertex step marks: bit i = the vertex belongs to pair i of the step.
+template <int CG> struct MarkOf { typedef uint16_t T; };
+template <> struct MarkOf<32> { typedef uint32_t T; };
+
 template <bool W16, int CG = kCG>
 __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsigned long long* __restrict__ keys,
                                              int lim, int max_verify, CommitStats* __restrict__ st,
@@ -232,7 +237,8 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
     unsigned char* used = smem;
     uint16_t* p16 = reinterpret_cast<uint16_t*>(smem + ((n + 15) & ~15));
     uint16_t* q16 = p16 + ((n + 8) & ~7);
-    uint16_t* mark = q16 + ((n + 8) & ~7);  // bit i set: vertex belongs to pair i of the step
+    typedef typename MarkOf<CG>::T MarkT;
+    MarkT* mark = reinterpret_cast<MarkT*>(q16 + ((n + 8) & ~7));  // bit i set: vertex belongs to pair i of the step
     __shared__ int s_lo[CG], s_hi[CG], s_d0[CG];
     __shared__ int s_corr[CG], s_cnt[CG], s_pre[CG + 1];
     __shared__ unsigned s_imask[CG];   // earlier pairs of the step G1-adjacent to this one
@@ -249,7 +255,8 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
     int gstep = 0;      // steps taken, the same in every CTA
     bool aborted = false;
     __shared__ __align__(8) unsigned long long s_cbar;   // the step mbarrier (nct arrivals per phase)
-    __shared__ int s_cpart[2][CG][3 + CG];              // this CTA's partial sums, by step parity
+    constexpr int kPart = (3 + CG + 3) & ~3;            // a pair's partials, padded to whole 16-byte words
+    __shared__ __align__(16) int s_cpart[2][CG][kPart];  // this CTA's partial sums, by step parity
     __shared__ int s_cc[CG][CG];   // s_cc[j][i]: change of pair j's delta if earlier pair i commits
     const uint32_t cbar = (uint32_t)__cvta_generic_to_shared(&s_cbar);
     if (nct > 1) {
@@ -343,8 +350,13 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
                 const int a = s_lo[lane], b = s_hi[lane];
                 len = s_inf[lane][1] + s_inf[lane][3] + s_inf[lane][5] + s_inf[lane][7];
                 s_corr[lane] = 0; s_cnt[lane] = 0; s_imask[lane] = 0;
-                atomicOr_u16(&mark[a], (uint16_t)(1u << lane));
-                atomicOr_u16(&mark[b], (uint16_t)(1u << lane));
+                if (sizeof(MarkT) == 2) {
+                    atomicOr_u16(reinterpret_cast<uint16_t*>(&mark[a]), (uint16_t)(1u << lane));
+                    atomicOr_u16(reinterpret_cast<uint16_t*>(&mark[b]), (uint16_t)(1u << lane));
+                } else {
+                    atomicOr(reinterpret_cast<unsigned*>(&mark[a]), 1u << lane);
+                    atomicOr(reinterpret_cast<unsigned*>(&mark[b]), 1u << lane);
+                }
             }
             __syncwarp();
             if (lane < cnt) {  // earlier pairs of the step that share a vertex: read off the marks
@@ -493,18 +505,24 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
                 aborted = true;
                 break;
             }
-            for (int t = tid; t < nct * cnt * (3 + CG); t += blockDim.x) {
-                // (c, j, k): field k of CTA c's partials of pair j (integer sums: any order)
-                const int c = t / (cnt * (3 + CG)), r = t - c * (cnt * (3 + CG));
-                const int j = r / (3 + CG), k = r - j * (3 + CG);
-                const uint32_t q = cluster_map((uint32_t)__cvta_generic_to_shared(&s_cpart[buf][j][k]), (uint32_t)c);
-                int v;
-                asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v) : "r"(q) : "memory");
-                if (!v) continue;
-                if (k == 0) atomicAdd(&s_corr[j], v);
-                else if (k == 1) atomicOr(&s_cnt[j], v);
-                else if (k == 2) atomicOr(&s_imask[j], (unsigned)v);
-                else atomicAdd(&s_cc[j][k - 3], v);
+            constexpr int kW = kPart / 4;   // 16-byte words per pair
+            for (int t = tid; t < nct * cnt * kW; t += blockDim.x) {
+                // (c, j, w): word w of CTA c's partials of pair j (integer sums: any order)
+                const int c = t / (cnt * kW), r = t - c * (cnt * kW);
+                const int j = r / kW, w = r - j * kW;
+                const uint32_t q = cluster_map((uint32_t)__cvta_generic_to_shared(&s_cpart[buf][j][4 * w]), (uint32_t)c);
+                int v[4];
+                asm volatile("ld.shared::cluster.v4.u32 {%0, %1, %2, %3}, [%4];"
+                             : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]) : "r"(q) : "memory");
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int k = 4 * w + u;
+                    if (!v[u] || k >= 3 + CG) continue;
+                    if (k == 0) atomicAdd(&s_corr[j], v[u]);
+                    else if (k == 1) atomicOr(&s_cnt[j], v[u]);
+                    else if (k == 2) atomicOr(&s_imask[j], (unsigned)v[u]);
+                    else atomicAdd(&s_cc[j][k - 3], v[u]);
+                }
             }
             __syncthreads();
         }
@@ -614,17 +632,18 @@ __host__ inline cudaError_t launch_commit_group(const DevView<W16>& g, const uns
                                                int max_verify, CommitStats* st, const int4* cinfo, int ctas,
                                                int* buf, size_t smem, cudaStream_t stream, int stall = 0);
 
-// Shared memory bytes of commit_group for n vertices.
-__host__ __device__ inline size_t commit_group_smem(int n) {
-    return (size_t)((n + 15) & ~15) + 3 * sizeof(uint16_t) * (size_t)((n + 8) & ~7);
+// Shared memory bytes of commit_group for n vertices (used flags, matching,
+// pre-move images, step marks of mark_bytes each).
+__host__ __device__ inline size_t commit_group_smem(int n, int mark_bytes = 2) {
+    return (size_t)((n + 15) & ~15) + (4 + mark_bytes) * (size_t)((n + 8) & ~7);
 }
 
-template <bool W16>
+template <bool W16, int CG = kCG>
 __global__ void __launch_bounds__(1024)
 k_commit_group(DevView<W16> g, const unsigned long long* __restrict__ keys, int lim, int max_verify,
                CommitStats* __restrict__ st, const int4* __restrict__ cinfo, CommitGrid grid) {
     extern __shared__ unsigned char smem[];
-    commit_group<W16>(g, keys, lim, max_verify, st, smem, cinfo, grid);
+    commit_group<W16, CG>(g, keys, lim, max_verify, st, smem, cinfo, grid);
 }
 
 template <bool W16>
@@ -638,12 +657,23 @@ __host__ inline cudaError_t launch_commit_group(const DevView<W16>& g, const uns
         k_commit_group<W16><<<1, 1024, smem, stream>>>(g, keys, lim, max_verify, st, cinfo, grid);
         return cudaGetLastError();
     }
+    // a cluster decides 32 pairs per step when 32-bit marks fit (n up to about
+    // 23,000), else 16
+    bool wide = false;
+    const size_t wsmem = commit_group_smem(g.n, 4);
+    if (cudaFuncSetAttribute(k_commit_group<W16, kCGWide>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsmem) ==
+        cudaSuccess) {
+        int per_sm = 0;
+        wide = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_commit_group<W16, kCGWide>, 1024, wsmem) ==
+                   cudaSuccess && per_sm >= 1;
+    }
+    cudaGetLastError();   // a refused attribute is not an error of this launch
     grid.nct = ctas;
     if ((e = cudaMemsetAsync(grid.err, 0, sizeof(int), stream)) != cudaSuccess) return e;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(ctas);
     cfg.blockDim = dim3(1024);
-    cfg.dynamicSmemBytes = smem;
+    cfg.dynamicSmemBytes = wide ? wsmem : smem;
     cfg.stream = stream;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -652,6 +682,7 @@ __host__ inline cudaError_t launch_commit_group(const DevView<W16>& g, const uns
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
+    if (wide) return cudaLaunchKernelEx(&cfg, k_commit_group<W16, kCGWide>, g, keys, lim, max_verify, st, cinfo, grid);
     return cudaLaunchKernelEx(&cfg, k_commit_group<W16>, g, keys, lim, max_verify, st, cinfo, grid);
 }
 
