@@ -423,6 +423,7 @@ extern "C" bm_status bm_set_mapping(bm_ctx* ctx, const int32_t* map) {
     CK(cudaMemcpyAsync(ctx->p, p.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
     CK(cudaMemcpyAsync(ctx->pinv, pinv.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
     ctx->mapped = true;
+    ctx->work_valid = false;   // row scheduling keys are estimated afresh for a new matching
     return compute_score(ctx, &ctx->score);
 }
 
@@ -524,13 +525,16 @@ bm_status stage_profit(bm_ctx* ctx) {
     if (ctx->nh && ctx->e2H)
         k_relabel<W16><<<rb, 256, 0, ctx->st>>>((const E*)ctx->ent2oH, (E*)ctx->ent2oHP, ctx->e2H, ctx->pinv);
     CK(cudaGetLastError());
-    // heaviest rows first
+    // heaviest rows first: each rebuild records its rows' work for the next
+    // one; after a new matching the estimate is computed afresh
+    if (!ctx->work_valid) {
+        k_row_work<W16><<<(n + 7) / 8, 256, 0, ctx->st>>>(g, ctx->is_hub, ctx->wkeys, ctx->wvals, nullptr);
+        CK(cudaGetLastError());
+    }
     CK(cudaMemsetAsync(ctx->work_sum, 0, sizeof(unsigned long long), ctx->st));
-    k_row_work<W16><<<(n + 7) / 8, 256, 0, ctx->st>>>(g, ctx->is_hub, ctx->wkeys, ctx->wvals, ctx->work_sum);
-    CK(cudaGetLastError());
     size_t tb = ctx->cub_bytes;
     CK(cub::DeviceRadixSort::SortPairsDescending(ctx->cub_tmp, tb, ctx->wkeys, ctx->wkeys_sorted,
-                                                 ctx->wvals, ctx->order, n, 0, 64, ctx->st));
+                                                 ctx->wvals, ctx->order, n, 0, 32, ctx->st));
     CK(cudaMemsetAsync(ctx->small, 0, sizeof(int), ctx->st));
     CK(cudaEventRecord(ctx->ev_hub, ctx->st));
     if (ctx->nh) {
@@ -569,8 +573,10 @@ bm_status stage_profit(bm_ctx* ctx) {
     if (per_sm < 1) { set_err(ctx, "profit kernel does not fit (n=%d)", n); return BM_E_INPUT; }
     CK(cudaEventRecord(ctx->ev[4], ctx->st));
     k_profit<W16><<<ctx->num_sms * per_sm, 512, smem, ctx->st>>>(g, ctx->order, ctx->small,
-                                                                ctx->nh ? ctx->is_hub : nullptr, kHubT);
+                                                                ctx->nh ? ctx->is_hub : nullptr, kHubT,
+                                                                ctx->wkeys, ctx->work_sum);
     CK(cudaGetLastError());
+    ctx->work_valid = true;
     CK(record_exact_mapping(ctx));
     CK(cudaEventRecord(ctx->ev[5], ctx->st));
     return BM_OK;

@@ -66,7 +66,8 @@ struct bm_ctx {
     long long dev_bytes = 0;
     cudaEvent_t ev[6] = {};
     cudaEvent_t uev[8] = {};       // bm_timer_* slots
-    unsigned long long* work_sum = nullptr;
+    unsigned long long* work_sum = nullptr;   // min terms of the last rebuild
+    bool work_valid = false;                  // wkeys hold the last rebuild's row work (scheduling keys)
     unsigned long long* part = nullptr;   // per-tile best partners (combine)
     // TMA-fed combine (n % 4 == 0): tensor map over S, S's diagonal, grid size
     alignas(64) CUtensorMap tmS;

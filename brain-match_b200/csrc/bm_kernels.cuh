@@ -113,10 +113,10 @@ __global__ void k_row_work(DevView<W16> g, const unsigned char* __restrict__ is_
         }
         for (int o = 16; o; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
         if (lane == 0) {
-            atomicAdd(total, (unsigned long long)w);   // min terms the row scatters
+            if (total) atomicAdd(total, (unsigned long long)w);   // min terms the row scatters
             w += (g.off1o[a + 1] - g.off1o[a]) + (g.off1i[a + 1] - g.off1i[a]);
             if (g.offs[a + 1] > g.offs[a]) w += g.n;
-            key[a] = (unsigned long long)w;
+            key[a] = (unsigned long long)min(w, 0xffffffffLL);   // 32-bit sort keys
             val[a] = a;
         }
     }
@@ -174,14 +174,22 @@ __device__ __forceinline__ void scatter_residual(int* acc, const typename Ent<W1
 
 // One profit row of S (all threads of the block call it together; it ends
 // with a barrier).  acc holds n+1 ints of shared memory.
+// With `work`, the row also records its scheduling key for the next rebuild
+// (its scattered min terms + its edges + n if it has self-loops, the
+// estimate k_row_work makes) in work[a], and adds its terms to *work_total.
 template <bool W16>
 __device__ __forceinline__ void profit_row(const DevView<W16>& g, int a, int* acc, int2* s_long, int* s_nlong,
-                                           const unsigned char* __restrict__ is_hub, int hub_thr) {
+                                           const unsigned char* __restrict__ is_hub, int hub_thr,
+                                           int* s_terms = nullptr, unsigned long long* work = nullptr,
+                                           unsigned long long* work_total = nullptr) {
     typedef Ent<W16> EN;
     typedef typename EN::T E;
     const int n = g.n;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
-    if (tid == 0) *s_nlong = 0;
+    if (tid == 0) {
+        *s_nlong = 0;
+        if (work) *s_terms = 0;
+    }
     // the row's scattered terms start from zero; with hubs, the tensor-core
     // hub terms already in S are added when the row is written back
     if ((n & 3) == 0) {
@@ -215,6 +223,11 @@ __device__ __forceinline__ void profit_row(const DevView<W16>& g, int a, int* ac
                 b0 = off[f];
                 b1 = off[f + 1];
             }
+        }
+        if (work) {   // the chunk's scattered terms
+            int c = kind ? b1 - b0 : 0;
+            for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+            if (lane == 0 && c) atomicAdd(s_terms, c);
         }
         const int cnt = min(32, (tot - base + nw - 1) / nw);
         for (int t = 0; t < cnt; t++) {
@@ -279,6 +292,12 @@ __device__ __forceinline__ void profit_row(const DevView<W16>& g, int a, int* ac
         }
     }
     __syncthreads();
+    if (work && tid == 0) {
+        const long long terms = *s_terms;
+        atomicAdd(work_total, (unsigned long long)terms);
+        long long w = terms + tot + (g.offs[a + 1] > g.offs[a] ? n : 0);
+        work[a] = (unsigned long long)min(w, 0xffffffffLL);
+    }
     int* row = g.S + (size_t)a * (size_t)n;
     if ((n & 3) == 0) {
         int4* r4 = reinterpret_cast<int4*>(row);
@@ -313,16 +332,17 @@ __device__ __forceinline__ void profit_row(const DevView<W16>& g, int a, int* ac
 template <bool W16>
 __global__ void __launch_bounds__(512)
 k_profit(DevView<W16> g, const int* __restrict__ order, int* __restrict__ counter,
-         const unsigned char* __restrict__ is_hub, int hub_thr) {
+         const unsigned char* __restrict__ is_hub, int hub_thr, unsigned long long* __restrict__ work,
+         unsigned long long* __restrict__ work_total) {
     extern __shared__ int acc[];
-    __shared__ int s_row, s_nlong;
+    __shared__ int s_row, s_nlong, s_terms;
     __shared__ int2 s_long[kLongQueue];  // (G2 vertex, w1 | kind << 31)
     for (;;) {
         if (threadIdx.x == 0) s_row = atomicAdd(counter, 1);
         __syncthreads();
         const int r = s_row;
         if (r >= g.n) break;
-        profit_row<W16>(g, order[r], acc, s_long, &s_nlong, is_hub, hub_thr);
+        profit_row<W16>(g, order[r], acc, s_long, &s_nlong, is_hub, hub_thr, &s_terms, work, work_total);
     }
 }
 
