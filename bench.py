@@ -288,24 +288,12 @@ def run_engine(args, g, world, rank, local, pg):
         except (OSError, ValueError):
             traffic = None
     terms = statistics.mean(s["min_terms"] for s in stats)
-    # the whole-sweep roofline: T_roof = max(compulsory bytes / HBM peak,
-    # algorithmic min+add / INT32 peak), with the reference's per-delta work
-    # 2 (d(a) + d(b)) summed over all pairs = 4 E (N - 1); the INT32 peak is
-    # measured live by the engine's microbenchmark (independent min+add pairs)
+    # the engine's own microbenchmark of shared-memory atomic adds at random
+    # addresses (the profit kernel's inner operation)
     try:
-        red_peak, minadd_peak = bm.measure_peaks(n)
+        red_peak, _ = bm.measure_peaks(n)
     except Exception:
-        red_peak, minadd_peak = None, None
-    sweep_roof = None
-    if minadd_peak:
-        ops = 4.0 * int(info["e1"]) * (n - 1)
-        t_roof = max(alg_bytes / (peak * 1e9), ops / minadd_peak)
-        t_meas = ms_max / args.steps / 1e3
-        sweep_roof = {"ops_per_sweep": ops, "int32_minadd_peak_per_s": minadd_peak,
-                      "smem_red_peak_per_s": red_peak, "t_roof_ms": 1e3 * t_roof, "t_sweep_ms": 1e3 * t_meas,
-                      "frac": t_roof / t_meas,
-                      "note": "above 1 because the sparse profit matrix skips the zero min terms "
-                              "that the per-pair formula counts"}
+        red_peak = None
     # k_profit against the roof that binds it: one shared-memory atomic add per
     # scattered min term, against the measured red.shared.add rate
     profit_atomics = None
@@ -370,7 +358,6 @@ def run_engine(args, g, world, rank, local, pg):
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "kernel": "k_profit", "kernel_ms": prof_ms, "alg_bytes": alg_bytes,
                          "min_terms": terms},
-            "sweep_roofline_int32": sweep_roof,
             "profit_smem_atomics": profit_atomics,
             "descent": descent,
             "cpu_baseline": cpu,
