@@ -147,6 +147,12 @@ static bm_status upload_dense(bm_ctx* ctx, const HostCSR& g2o, const HostCSR& g2
                           cudaMemcpyHostToDevice));
         }
     }
+    std::vector<int> diag(n1, 0);   // G2 self-loops: W2[f][f]
+    for (int f = 0; f < n; f++)
+        for (int i = g2o.off[f]; i < g2o.off[f + 1]; i++)
+            if (g2o.id[i] == f) diag[f] = std::min(g2o.w[i], clamp2);
+    CK(dalloc(ctx, &ctx->W2D, n1 * sizeof(int)));
+    CK(cudaMemcpy(ctx->W2D, diag.data(), n1 * sizeof(int), cudaMemcpyHostToDevice));
     return BM_OK;
 }
 
@@ -154,6 +160,7 @@ static void free_ctx(bm_ctx* c) {
     if (!c) return;
     for (void* b : {(void*)c->off2oH, c->ent2oH, c->ent2oHP}) if (b) cudaFree(b);
     if (c->W2T) cudaFree(c->W2T);
+    if (c->W2D) cudaFree(c->W2D);
     void* bufs[] = {c->off1o, c->off1i, c->off2o, c->off2i, c->offs, c->selfw, c->ent1o, c->ent1i,
                     c->ent2o, c->ent2i, c->ent1oP, c->ent1iP, c->ent2oP, c->ent2iP, c->W2, c->p,
                     c->pinv, c->S, c->rowbest, c->ckeys, c->ckeys_sorted, c->wkeys, c->wkeys_sorted,

@@ -132,7 +132,7 @@ __global__ void k_corner(DevView<W16> g, const int* __restrict__ pm, const int* 
         if (pS[a] != g.p[a]) return;  // the source moved too: done from its out-list
     }
     const int pa = pm[a], pb = pm[b];
-    const int c = corner_term(x, g.w2(pa, pb), g.w2(pb, pa), g.w2(pa, pa), g.w2(pb, pb));
+    const int c = corner_term(x, g.w2(pa, pb), g.w2t(pb, pa), g.w2d(pa), g.w2d(pb));
     if (c) atomicAdd(&g.S[(size_t)a * n + b], sign * c);
 }
 

@@ -35,6 +35,7 @@ struct bm_ctx {
     long long e2H = 0;
     void* W2 = nullptr;
     void* W2T = nullptr;
+    int* W2D = nullptr;            // W2's diagonal, n+1 entries (entry n = 0)
     int *p = nullptr, *pinv = nullptr;
     int* S = nullptr;
     unsigned long long* rowbest = nullptr;
@@ -125,6 +126,7 @@ inline DevView<W16> view(bm_ctx* c) {
     g.off2oH = c->off2oH; g.ent2oHP = (E*)c->ent2oHP;
     g.W2 = (const D*)c->W2;
     g.W2T = (const D*)c->W2T;
+    g.W2D = c->W2D;
     g.p = c->p; g.pinv = c->pinv;
     g.S = c->S;
     return g;

@@ -63,6 +63,7 @@ template <bool W16> struct DevView {
     const int* off2oH; E* ent2oHP;      // G2 out-entries above the hub threshold, mapped through pinv
     const D* W2;                        // dense (n+1)^2, row/col n zero
     const D* W2T;                       // its transpose (columns of W2 read as rows)
+    const int* W2D;                     // its diagonal W2[f][f], f = 0..n
     int* p; int* pinv;                  // n+1 entries, [n] = n
     int* S;                             // n*n profit matrix
     __device__ __forceinline__ int w2(int f, int g) const {
@@ -72,6 +73,8 @@ template <bool W16> struct DevView {
     __device__ __forceinline__ int w2t(int f, int g) const {
         return (int)W2T[(size_t)g * (size_t)(n + 1) + (size_t)f];
     }
+    // same value as w2(f, f)
+    __device__ __forceinline__ int w2d(int f) const { return W2D[f]; }
 };
 
 __device__ __forceinline__ int imin(int a, int b) { return a < b ? a : b; }
@@ -268,12 +271,13 @@ __device__ __forceinline__ void profit_row(const DevView<W16>& g, int a, int* ac
     // corner corrections for every G1 edge a->b
     {
         const int pa = g.p[a];
+        const int dpa = g.w2d(pa);
         for (int j = tid; j < lo; j += blockDim.x) {
             const int b = EN::id(g.ent1o[so + j]);
             const E ep = g.ent1oP[so + j];
             const int pb = EN::id(ep), x = EN::w(ep);
-            const int c = imin(x, g.w2(pa, pb)) + imin(x, g.w2(pb, pa))
-                        - imin(x, g.w2(pa, pa)) - imin(x, g.w2(pb, pb));
+            const int c = imin(x, g.w2(pa, pb)) + imin(x, g.w2t(pb, pa))
+                        - imin(x, dpa) - imin(x, g.w2d(pb));
             if (c) atomicAdd(&acc[b], c);
         }
     }
@@ -284,7 +288,7 @@ __device__ __forceinline__ void profit_row(const DevView<W16>& g, int a, int* ac
             __syncthreads();
             for (int b = tid; b < n; b += blockDim.x) {
                 const int pb = g.p[b];
-                const int d = g.w2(pb, pb);
+                const int d = g.w2d(pb);
                 int t = 0;
                 for (int q = q0; q < q1; q++) t += imin(g.selfw[q], d);
                 acc[b] += t;
