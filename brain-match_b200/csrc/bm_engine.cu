@@ -328,15 +328,18 @@ extern "C" bm_status bm_create(bm_ctx** out, int32_t n, int64_t e1, const int32_
         CK(dalloc(ctx, &ctx->hub_err, sizeof(int)));
         CK(cudaMemset(ctx->hub_err, 0, sizeof(int)));
         if (!(flags & BM_FLAG_NO_HUB_GEMM)) {
-            // hubs: G1 vertices of out-degree >= max(64, n/8), at most kHubMaxHubs,
+            // hubs: G1 vertices of out-degree >= max(64, n/9), at most kHubMaxHubs,
             // topped up by the next-largest out-degrees to a multiple of 16 so the
-            // GEMM depth (hubs x thresholds) is a multiple of 128 bytes
+            // GEMM depth (hubs x thresholds) is a multiple of 128 bytes.  A hub
+            // adds n^2 x kHubT operations to the GEMM and takes out about
+            // deg^2 scattered terms once hubs are matched to hubs; at
+            // n = 18,524 the sweep is fastest near 256 hubs (out-degree >= n/9)
             std::vector<int> byd(n);
             for (int v = 0; v < n; v++) byd[v] = v;
             std::stable_sort(byd.begin(), byd.end(), [&](int x, int y) {
                 return (g1o.off[x + 1] - g1o.off[x]) > (g1o.off[y + 1] - g1o.off[y]);
             });
-            const int thr = std::max(64, n / 8);
+            const int thr = std::max(64, n / 9);
             int nh = 0;
             while (nh < std::min(n, kHubMaxHubs) && g1o.off[byd[nh] + 1] - g1o.off[byd[nh]] >= thr) nh++;
             if (nh > 0) {

@@ -21,7 +21,7 @@
 namespace bm {
 
 constexpr int kHubT = 8;          // thresholds per hub
-constexpr int kHubMaxHubs = 128;  // K = 1024
+constexpr int kHubMaxHubs = 256;  // K up to 2048
 constexpr int kGemmM = 128, kGemmN = 256, kGemmKC = 128;  // tile rows, cols, K bytes per stage
 constexpr int kGemmStages = 2;
 constexpr int kGemmThreads = 128;

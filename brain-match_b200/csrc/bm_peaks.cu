@@ -5,8 +5,9 @@
 // address of an (n+1)-int row.  bm_measure_peaks times, on the current
 // device, (1) that access pattern at full occupancy with no global traffic
 // (random addresses over an n-int shared array, 3 CTAs x 512 threads per SM,
-// like the profit kernel) and (2) independent int32 min+add pairs, the
-// operation count the dense formulation of the sweep is quoted in.
+// like the profit kernel, two integer operations of address arithmetic per
+// atomic) and (2) independent int32 min+add pairs, the operation count the
+// dense formulation of the sweep is quoted in.
 #include <cuda_runtime.h>
 #include <cstdint>
 #include "bm.h"
@@ -17,16 +18,23 @@ __global__ void __launch_bounds__(512) k_peak_red(int n, int iters, unsigned see
     extern __shared__ int acc[];
     for (int i = threadIdx.x; i <= n; i += blockDim.x) acc[i] = 0;
     __syncthreads();
-    unsigned x = seed ^ (blockIdx.x * 9781u + threadIdx.x * 6271u);
+    // addresses uniform over the largest power of two <= n, from four
+    // independent LCG streams: two integer operations per atomic, so the
+    // shared-memory atomic unit (not the address arithmetic) is what is timed
+    int lg = 0;
+    while ((2 << lg) <= n) lg++;
+    const unsigned sh = 32u - (unsigned)lg;
+    unsigned x0 = seed ^ (blockIdx.x * 9781u + threadIdx.x * 6271u), x1 = x0 * 3u + 1u, x2 = x0 * 5u + 7u,
+             x3 = x0 * 9u + 3u;
     for (int it = 0; it < iters; it++) {
-        // four independent xorshift addresses per round
-        unsigned a0 = x, a1 = x * 747796405u + 2891336453u, a2 = a1 * 747796405u + 2891336453u,
-                 a3 = a2 * 747796405u + 2891336453u;
-        x = a3 * 747796405u + 2891336453u;
-        atomicAdd(&acc[(a0 >> 8) % (unsigned)n], 1);
-        atomicAdd(&acc[(a1 >> 8) % (unsigned)n], 2);
-        atomicAdd(&acc[(a2 >> 8) % (unsigned)n], 3);
-        atomicAdd(&acc[(a3 >> 8) % (unsigned)n], 4);
+        x0 = x0 * 1664525u + 1013904223u;
+        x1 = x1 * 1664525u + 1013904223u;
+        x2 = x2 * 1664525u + 1013904223u;
+        x3 = x3 * 1664525u + 1013904223u;
+        atomicAdd(&acc[x0 >> sh], 1);
+        atomicAdd(&acc[x1 >> sh], 2);
+        atomicAdd(&acc[x2 >> sh], 3);
+        atomicAdd(&acc[x3 >> sh], 4);
     }
     __syncthreads();
     if (threadIdx.x == 0) atomicAdd(sink, acc[blockIdx.x % n]);
