@@ -148,6 +148,7 @@ def lib():
         L.bm_batch_get_mappings.argtypes = [vp, vp]
         L.bm_batch_scores.argtypes = [vp, vp]
         L.bm_batch_autotune.argtypes = [vp, C.POINTER(i32), C.POINTER(i32)]
+        L.bm_batch_set_schedule.argtypes = [vp, i32, i32, i32]
         L.bm_batch_sweeps.argtypes = [vp, i32, C.POINTER(SweepOpts), vp, C.POINTER(C.c_float)]
         L.bm_batch_info.argtypes = [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(i64), C.POINTER(i32), C.POINTER(i32)]
         L.bm_mlp_param_count.restype = i64
@@ -486,6 +487,10 @@ class Batch:
         a, b = C.c_int32(), C.c_int32()
         self._chk(lib().bm_batch_autotune(self.h, C.byref(a), C.byref(b)))
         return a.value, b.value
+
+    def set_schedule(self, persistent, profit_threads=512, combine_tile=64):
+        """persistent: one launch per sweep; else the launch sequence."""
+        self._chk(lib().bm_batch_set_schedule(self.h, int(bool(persistent)), int(profit_threads), int(combine_tile)))
 
     def sweeps(self, k, max_candidates=0, max_verify=-1):
         o = SweepOpts(max_candidates, max_verify)

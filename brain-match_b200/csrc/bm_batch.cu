@@ -3,18 +3,20 @@
 //
 // Each instance is an ordinary context (bm_create: same preprocessing, same
 // storage, same exact arithmetic); the batch adds device tables of the
-// instances' buffers and batched kernels that run the shared per-row,
-// per-tile and per-instance bodies of the single-instance path:
-//   relabel (all lists of all instances)  -> row work + one LPT sort over all
-//   (instance, row) items -> one persistent profit-row launch over every item
-//   -> one combine launch over every (instance, tile) item -> reduce ->
-//   candidates -> one segmented sort -> one commit launch (a CTA per instance)
-//   -> per-instance statistics.
+// instances' buffers and runs the shared per-row, per-tile and per-instance
+// bodies of the single-instance path in one of two schedules:
+//   * the launch sequence: relabel (all lists of all instances) -> row work +
+//     one LPT sort over all (instance, row) items -> one persistent
+//     profit-row launch over every item -> one combine launch over every
+//     (instance, tile) item -> reduce -> candidates -> one segmented sort ->
+//     one commit launch (a CTA per instance);
+//   * one persistent launch (k_b_sweep): the same phases in one cooperative
+//     grid behind grid barriers, the candidate sort in shared memory.
 // One sweep of the whole batch is captured once as a CUDA graph and replayed.
-// The launch shapes (profit-row block size, combine tile) are picked by
-// bm_batch_autotune, which times the candidates on the batch itself; results
-// do not depend on the choice.  Hub tensor-core terms are not used here: the
-// instances are built with BM_FLAG_NO_HUB_GEMM.
+// The schedule and its launch shapes (profit-row block size, combine tile)
+// are picked by bm_batch_autotune, which times the candidates on the batch
+// itself; results do not depend on the choice.  Hub tensor-core terms are
+// not used here: the instances are built with BM_FLAG_NO_HUB_GEMM.
 #include <cstdio>
 #include <cstring>
 #include <vector>
@@ -22,6 +24,7 @@
 #include <cuda_runtime.h>
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_segmented_radix_sort.cuh>
+#include <cub/block/block_radix_sort.cuh>
 #include "bm.h"
 #include "bm_internal.cuh"
 #include "bm_select.cuh"
@@ -194,6 +197,213 @@ k_b_commit(const DevView<W16>* __restrict__ views, const BatchInst* __restrict__
     }
 }
 
+// ---------------------------------------------------------------------------
+// One batch sweep as one persistent launch: a cooperative grid of one
+// 1024-thread CTA per SM runs the phases above back to back, separated by a
+// bounded grid barrier:
+//   relabel -> profit rows (four 256-thread groups per CTA, an (instance,
+//   row) item each from a global counter) -> combine (four groups, an
+//   (instance, tile) item each) -> reduce ->
+//   candidates -> per instance (a CTA each): block radix sort of its
+//   candidate keys in shared memory, then the set commit.
+// Every phase's shared memory is the same dynamic buffer.  Row order does not
+// matter for the result (integer sums), so rows are taken in index order.
+constexpr int kBThreads = 1024;
+constexpr int kBSortItems = 8;                           // candidate keys per thread
+constexpr int kBSortMax = kBThreads * kBSortItems;       // instances up to 8,192 vertices
+constexpr unsigned kBSpinLimit = 1u << 24;               // polls of one grid-barrier wait (~1 s)
+typedef cub::BlockRadixSort<unsigned long long, kBThreads, kBSortItems> BSort;
+
+template <bool W16>
+struct BSweepArgs {
+    const DevView<W16>* views;
+    const BatchInst* inst;
+    const int* row_base;
+    const long long* tile_base;
+    const long long* ebase;   // 4 count + 1: list segments laid end to end
+    const typename Ent<W16>::T* const* lists;
+    int nb, total;
+    long long total_tiles;
+    int acc_w;             // ints per row accumulator (max n + 1, rounded up to 4)
+    int* counter;          // profit-row items taken
+    unsigned* bar;         // grid barrier: arrivals, generation, error
+    int max_scan, max_verify;
+    CommitStats* st;
+    long long* acc_delta;
+    long long* acc_commits;
+};
+
+__device__ __forceinline__ unsigned b_ld_acquire(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Grid-wide barrier of the co-resident CTAs.  A wait that runs out sets the
+// error word (bar[2]); every CTA leaves at its next barrier.  Returns false
+// once the error word is set.
+__device__ bool b_grid_barrier(unsigned* bar) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        __threadfence();
+        const unsigned gen = b_ld_acquire(&bar[1]);
+        if (atomicAdd(&bar[0], 1u) == gridDim.x - 1) {
+            atomicExch(&bar[0], 0u);
+            __threadfence();
+            atomicAdd(&bar[1], 1u);
+        } else {
+            unsigned it = 0;
+            while (b_ld_acquire(&bar[1]) == gen) {
+                if (b_ld_acquire(&bar[2]) || ++it > kBSpinLimit) {
+                    atomicExch(&bar[2], 1u);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        s_ok = ok && !b_ld_acquire(&bar[2]);
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+__device__ __forceinline__ void b_group_sync(int grp) {
+    asm volatile("bar.sync %0, 256;" :: "r"(grp + 1) : "memory");
+}
+
+template <bool W16, int T>
+__global__ void __launch_bounds__(kBThreads, 1) k_b_sweep(BSweepArgs<W16> a) {
+    typedef Ent<W16> EN;
+    extern __shared__ __align__(16) unsigned char bsm[];
+    const int tid = threadIdx.x;
+    const long long gt = (long long)blockIdx.x * blockDim.x + tid, gs = (long long)gridDim.x * blockDim.x;
+    // relabel every instance's lists (G1 through p, G2 through pinv): the
+    // lists laid end to end (segment 4b + lst starts at ebase[4b + lst]), each
+    // CTA one contiguous range of that
+    {
+        const long long tot = a.ebase[4 * a.nb];
+        const long long per = (tot + gridDim.x - 1) / gridDim.x;
+        const long long lo = (long long)blockIdx.x * per, hi = min(tot, lo + per);
+        for (int sg = 0; sg < 4 * a.nb && lo < hi; sg++) {
+            const long long s0 = max(lo, a.ebase[sg]), s1 = min(hi, a.ebase[sg + 1]);
+            if (s0 >= s1) continue;
+            const int b = sg >> 2, lst = sg & 3;
+            const DevView<W16>& g = a.views[b];
+            const typename EN::T* in = a.lists[sg];
+            typename EN::T* out = lst == 0 ? g.ent1oP : lst == 1 ? g.ent1iP : lst == 2 ? g.ent2oP : g.ent2iP;
+            const int* map = lst < 2 ? g.p : g.pinv;
+            for (long long i = s0 - a.ebase[sg] + tid; i < s1 - a.ebase[sg]; i += blockDim.x) {
+                const typename EN::T e = in[i];
+                out[i] = EN::make(map[EN::id(e)], EN::w(e));
+            }
+        }
+    }
+    if (blockIdx.x == 0 && tid == 0) *a.counter = 0;   // read only after the barrier
+    if (!b_grid_barrier(a.bar)) return;
+    // profit rows: four groups of 256 threads, each with its own row
+    // accumulator, take (instance, row) items one at a time
+    {
+        const int grp = tid >> 8, gtid = tid & 255;
+        int* acc = reinterpret_cast<int*>(bsm) + (size_t)grp * a.acc_w;
+        __shared__ int s_item[4], s_nlong[4];
+        __shared__ int2 s_long[4][kLongQueue];
+        for (;;) {
+            if (gtid == 0) s_item[grp] = atomicAdd(a.counter, 1);
+            b_group_sync(grp);
+            const int r = s_item[grp];
+            if (r >= a.total) break;
+            const int b = find_inst(a.row_base, a.nb, r);
+            const DevView<W16> g = a.views[b];
+            profit_row_on<W16, 256>(g, r - a.row_base[b], acc, s_long[grp], &s_nlong[grp], nullptr, 0, nullptr,
+                                    nullptr, nullptr, [grp] { b_group_sync(grp); });
+        }
+    }
+    if (!b_grid_barrier(a.bar)) return;
+    // combine: four groups of 256 threads, an (instance, tile) item each
+    {
+        const int grp = tid >> 8, gtid = tid & 255;
+        CombineSmem<T>& cs = reinterpret_cast<CombineSmem<T>*>(bsm)[grp];
+        for (long long it = (long long)blockIdx.x * 4 + grp; it < a.total_tiles; it += 4LL * gridDim.x) {
+            const int b = find_inst_ll(a.tile_base, a.nb, it);
+            const BatchInst I = a.inst[b];
+            long long t = it - a.tile_base[b];
+            int ti = 0;
+            while (t >= I.tiles - ti) { t -= I.tiles - ti; ti++; }
+            const int tj = ti + (int)t;
+            combine_tile_on<T>(I.S, I.n, ti, tj, I.part, nullptr, cs, gtid, [grp] { b_group_sync(grp); });
+            b_group_sync(grp);   // cs is rewritten by the group's next item
+        }
+    }
+    if (!b_grid_barrier(a.bar)) return;
+    // row bests: max over the tile partials
+    for (long long x = gt; x < a.total; x += gs) {
+        const int b = find_inst(a.row_base, a.nb, (int)x);
+        const BatchInst I = a.inst[b];
+        const int xi = (int)x - a.row_base[b];
+        unsigned long long k = 0;
+        for (int t = 0; t < I.tiles; t++) k = kmax(k, I.part[(size_t)t * I.n + xi]);
+        I.rowbest[xi] = k;
+    }
+    if (!b_grid_barrier(a.bar)) return;
+    // candidate keys (the single-instance rule, k_candidates)
+    for (long long x = gt; x < a.total; x += gs) {
+        const int b = find_inst(a.row_base, a.nb, (int)x);
+        const BatchInst I = a.inst[b];
+        const int xa = (int)x - a.row_base[b];
+        const unsigned long long k = I.rowbest[xa];
+        unsigned long long out = ~0ull;
+        if (k) {
+            const int d = (int)((unsigned)(k >> 32) - 0x80000000u);
+            const int q = (int)(~(unsigned)(k & 0xffffffffu));
+            if (d > 0) {
+                const unsigned long long kb = I.rowbest[q];
+                const int qq = (int)(~(unsigned)(kb & 0xffffffffu));
+                const bool mutual = (kb != 0) && (qq == xa);
+                if (!mutual || xa < q) {
+                    const int lo = xa < q ? xa : q, hi = xa < q ? q : xa;
+                    out = ((unsigned long long)(0x7fffffffu - (unsigned)d) << 32) |
+                          ((unsigned long long)lo << 16) | (unsigned long long)hi;
+                }
+            }
+        }
+        I.keys[xa] = out;
+    }
+    if (!b_grid_barrier(a.bar)) return;
+    // per instance: sort its candidates in shared memory, then the set commit
+    for (int b = blockIdx.x; b < a.nb; b += gridDim.x) {
+        const BatchInst I = a.inst[b];
+        {
+            typename BSort::TempStorage& ts = *reinterpret_cast<typename BSort::TempStorage*>(bsm);
+            unsigned long long k[kBSortItems];
+#pragma unroll
+            for (int q = 0; q < kBSortItems; q++) {
+                const int i = tid * kBSortItems + q;
+                k[q] = i < I.n ? I.keys[i] : ~0ull;
+            }
+            BSort(ts).Sort(k);
+#pragma unroll
+            for (int q = 0; q < kBSortItems; q++) {
+                const int i = tid * kBSortItems + q;
+                if (i < I.n) I.keys_sorted[i] = k[q];
+            }
+        }
+        __syncthreads();
+        const DevView<W16> g = a.views[b];
+        const int lim = (a.max_scan > 0 && a.max_scan < I.n) ? a.max_scan : I.n;
+        commit_group<W16, kCGBatch>(g, I.keys_sorted, lim, a.max_verify, &a.st[b], bsm);
+        __syncthreads();
+        if (tid == 0) {
+            a.acc_delta[b] += a.st[b].total_delta;
+            a.acc_commits[b] += a.st[b].committed;
+        }
+        __syncthreads();
+    }
+}
+
 }  // namespace
 
 struct bm_batch {
@@ -211,6 +421,7 @@ struct bm_batch {
     int* row_base = nullptr;              // count+1
     long long* tile_base = nullptr;       // count+1
     long long *e1 = nullptr, *e2 = nullptr;
+    long long* ebase = nullptr;           // 4 count + 1: the lists laid end to end (persistent relabel)
     void** lists = nullptr;               // 4 per instance: ent1o, ent1i, ent2o, ent2i
     unsigned long long *wkeys = nullptr, *wkeys_sorted = nullptr, *ckeys = nullptr, *ckeys_sorted = nullptr;
     int *wvals = nullptr, *order = nullptr;
@@ -222,6 +433,12 @@ struct bm_batch {
     long long *acc_delta = nullptr, *acc_commits = nullptr;
     long long total_tiles = 0;
     std::vector<BatchInst> hinst;
+    // schedules: one persistent launch per sweep (k_b_sweep, possible when
+    // every instance's candidates fit its in-kernel sort) or the launch
+    // sequence above; the autotuner times both and keeps the faster
+    bool can_persist = false, use_persist = false;
+    size_t psmem = 0;
+    unsigned* gbar = nullptr;             // its grid barrier
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int graph_max_scan = 0, graph_max_verify = -1;
@@ -229,6 +446,9 @@ struct bm_batch {
 };
 
 static thread_local char g_batch_create_err[512];
+
+template <bool W16>
+static bm_status persistent_setup(bm_batch* B);
 
 #define BK(call)                                                                         \
     do {                                                                                 \
@@ -246,7 +466,7 @@ static void batch_free(bm_batch* B) {
     if (B->graph) cudaGraphDestroy(B->graph);
     void* bufs[] = {B->views, B->inst, B->row_base, B->tile_base, B->e1, B->e2, B->lists, B->wkeys,
                     B->wkeys_sorted, B->ckeys, B->ckeys_sorted, B->wvals, B->order, B->rowbest, B->part,
-                    B->cub_tmp, B->counter, B->cstats, B->acc_delta, B->acc_commits};
+                    B->cub_tmp, B->counter, B->cstats, B->acc_delta, B->acc_commits, B->gbar, B->ebase};
     for (void* p : bufs) if (p) cudaFree(p);
     if (B->ev0) cudaEventDestroy(B->ev0);
     if (B->ev1) cudaEventDestroy(B->ev1);
@@ -295,6 +515,11 @@ static bm_status batch_tables(bm_batch* B) {
     BK(cudaMalloc(&B->e2, B->count * sizeof(long long)));
     BK(cudaMemcpy(B->e1, e1.data(), B->count * sizeof(long long), cudaMemcpyHostToDevice));
     BK(cudaMemcpy(B->e2, e2.data(), B->count * sizeof(long long), cudaMemcpyHostToDevice));
+    std::vector<long long> eb(4 * (size_t)B->count + 1, 0);
+    for (int i = 0; i < B->count; i++)
+        for (int l = 0; l < 4; l++) eb[4 * i + l + 1] = eb[4 * i + l] + (l < 2 ? e1[i] : e2[i]);
+    BK(cudaMalloc(&B->ebase, eb.size() * sizeof(long long)));
+    BK(cudaMemcpy(B->ebase, eb.data(), eb.size() * sizeof(long long), cudaMemcpyHostToDevice));
     return BM_OK;
 }
 
@@ -391,6 +616,10 @@ extern "C" bm_status bm_batch_create(bm_batch** out, int32_t count, const int32_
         }
         bm_status s2 = B->w16 ? batch_tables<true>(B) : batch_tables<false>(B);
         if (s2) return s2;
+        BK(cudaMalloc(&B->gbar, 4 * sizeof(unsigned)));
+        BK(cudaMemset(B->gbar, 0, 4 * sizeof(unsigned)));
+        s2 = B->w16 ? persistent_setup<true>(B) : persistent_setup<false>(B);
+        if (s2) return s2;
         return batch_tiles(B);
     };
     s = body();
@@ -427,6 +656,79 @@ extern "C" bm_status bm_batch_scores(bm_batch* B, int64_t* scores) {
         bm_status s = bm_score(B->ctx[i], &scores[i]);
         if (s) { snprintf(B->err, sizeof B->err, "instance %d: %.480s", i, B->ctx[i]->err); return s; }
     }
+    return BM_OK;
+}
+
+// Shared memory of k_b_sweep: the largest of its phases' needs.
+template <int T>
+static size_t persistent_smem(int max_n) {
+    size_t m = 4 * (size_t)((max_n + 1 + 3) & ~3) * sizeof(int);         // four profit rows
+    m = std::max(m, 4 * sizeof(CombineSmem<T>));                           // four combine groups
+    m = std::max(m, sizeof(typename BSort::TempStorage));                  // the candidate sort
+    m = std::max(m, commit_group_smem(max_n));                             // the set commit
+    return (m + 15) & ~(size_t)15;
+}
+
+template <bool W16, int T>
+static bool persistent_fits(bm_batch* B, size_t* smem) {
+    const size_t sm = persistent_smem<T>(B->max_n);
+    if (cudaFuncSetAttribute(k_b_sweep<W16, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_b_sweep<W16, T>, kBThreads, sm) != cudaSuccess ||
+        per_sm < 1) {
+        cudaGetLastError();
+        return false;
+    }
+    *smem = sm;
+    return true;
+}
+
+// Whether every batch sweep can be one persistent launch: the instances'
+// candidates fit the in-kernel sort and the kernel fits one CTA per SM with
+// either combine tile.
+template <bool W16>
+static bm_status persistent_setup(bm_batch* B) {
+    size_t s32 = 0, s64 = 0;
+    B->can_persist = B->max_n <= kBSortMax && persistent_fits<W16, 32>(B, &s32) && persistent_fits<W16, 64>(B, &s64);
+    B->psmem = std::max(s32, s64);
+    return BM_OK;
+}
+
+template <bool W16>
+static bm_status enqueue_persistent(bm_batch* B, int max_scan, int max_verify) {
+    BSweepArgs<W16> a;
+    a.views = (const DevView<W16>*)B->views;
+    a.inst = B->inst;
+    a.row_base = B->row_base;
+    a.tile_base = B->tile_base;
+    a.ebase = B->ebase;
+    a.lists = (const typename Ent<W16>::T* const*)B->lists;
+    a.nb = B->count;
+    a.total = B->total;
+    a.total_tiles = B->total_tiles;
+    a.acc_w = (B->max_n + 1 + 3) & ~3;
+    a.counter = B->counter;
+    a.bar = B->gbar;
+    a.max_scan = max_scan;
+    a.max_verify = max_verify;
+    a.st = B->cstats;
+    a.acc_delta = B->acc_delta;
+    a.acc_commits = B->acc_commits;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(B->ctx[0]->num_sms);
+    cfg.blockDim = dim3(kBThreads);
+    cfg.dynamicSmemBytes = B->tile == 32 ? persistent_smem<32>(B->max_n) : persistent_smem<64>(B->max_n);
+    cfg.stream = B->st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (B->tile == 32) BK(cudaLaunchKernelEx(&cfg, k_b_sweep<W16, 32>, a));
+    else BK(cudaLaunchKernelEx(&cfg, k_b_sweep<W16, 64>, a));
     return BM_OK;
 }
 
@@ -482,6 +784,9 @@ static bm_status enqueue_select_commit(bm_batch* B, int max_scan, int max_verify
 }
 
 static bm_status enqueue_sweep(bm_batch* B, int max_scan, int max_verify) {
+    if (B->use_persist)
+        return B->w16 ? enqueue_persistent<true>(B, max_scan, max_verify)
+                      : enqueue_persistent<false>(B, max_scan, max_verify);
     bm_status s = B->w16 ? enqueue_eval<true>(B) : enqueue_eval<false>(B);
     if (s) return s;
     return B->w16 ? enqueue_select_commit<true>(B, max_scan, max_verify)
@@ -492,36 +797,86 @@ extern "C" bm_status bm_batch_autotune(bm_batch* B, int32_t* profit_threads, int
     if (!B) return BM_E_INPUT;
     for (bm_ctx* c : B->ctx)
         if (!c->mapped) { snprintf(B->err, sizeof B->err, "bm_batch_autotune: mappings not set"); return BM_E_STATE; }
-    const int pt[2] = {256, 512}, tl[2] = {32, 64};
-    float best = 1e30f;
-    int bp = 512, bt = 64;
-    for (int i = 0; i < 2; i++)
-        for (int j = 0; j < 2; j++) {
-            B->profit_threads = pt[i];
-            B->tile = tl[j];
-            bm_status s = batch_tiles(B);
+    // candidate schedules: the persistent launch with either combine tile,
+    // and the launch sequence with profit blocks of 256 or 512 threads and
+    // either tile; each is timed on whole sweeps of the batch itself from the
+    // same matchings, restored afterwards (results never depend on the choice)
+    struct Sched { bool persist; int threads, tile; };
+    std::vector<Sched> cand;
+    if (B->can_persist) { cand.push_back({true, kBThreads, 32}); cand.push_back({true, kBThreads, 64}); }
+    for (int pt : {256, 512})
+        for (int tl : {32, 64}) cand.push_back({false, pt, tl});
+    std::vector<std::vector<int32_t>> saved(B->count);
+    for (int i = 0; i < B->count; i++) {
+        saved[i].resize((size_t)B->ctx[i]->n + 1);
+        bm_status s = bm_get_mapping(B->ctx[i], saved[i].data());
+        if (s) return s;
+    }
+    auto restore = [&]() -> bm_status {
+        for (int i = 0; i < B->count; i++) {
+            bm_status s = bm_set_mapping(B->ctx[i], saved[i].data());
             if (s) return s;
-            float ms = 0, tot = 0;
-            for (int rep = 0; rep < 3; rep++) {
-                BK(cudaEventRecord(B->ev0, B->st));
-                s = B->w16 ? enqueue_eval<true>(B) : enqueue_eval<false>(B);
-                if (s) return s;
-                BK(cudaEventRecord(B->ev1, B->st));
-                BK(cudaEventSynchronize(B->ev1));
-                BK(cudaEventElapsedTime(&ms, B->ev0, B->ev1));
-                if (rep) tot += ms;  // first repetition warms up
-            }
-            if (tot < best) { best = tot; bp = pt[i]; bt = tl[j]; }
         }
-    B->profit_threads = bp;
-    B->tile = bt;
-    bm_status s = batch_tiles(B);
+        return BM_OK;
+    };
+    float best = 1e30f;
+    Sched pick = cand[0];
+    for (const Sched& c : cand) {
+        B->use_persist = c.persist;
+        B->profit_threads = c.threads;
+        B->tile = c.tile;
+        bm_status s = batch_tiles(B);
+        if (s) return s;
+        // the second and third sweep from the saved matchings (the first
+        // warms up and has a descent's first, commit-heavy candidate set)
+        if ((s = restore())) return s;
+        if ((s = enqueue_sweep(B, 0, -1))) return s;
+        BK(cudaEventRecord(B->ev0, B->st));
+        for (int rep = 0; rep < 2; rep++)
+            if ((s = enqueue_sweep(B, 0, -1))) return s;
+        BK(cudaEventRecord(B->ev1, B->st));
+        BK(cudaEventSynchronize(B->ev1));
+        float tot = 0;
+        BK(cudaEventElapsedTime(&tot, B->ev0, B->ev1));
+        if (tot < best) { best = tot; pick = c; }
+    }
+    bm_status s = restore();
     if (s) return s;
+    B->use_persist = pick.persist;
+    B->profit_threads = pick.threads;
+    B->tile = pick.tile;
+    if ((s = batch_tiles(B))) return s;
     B->tuned = true;
     if (B->exec) { cudaGraphExecDestroy(B->exec); B->exec = nullptr; }
     if (B->graph) { cudaGraphDestroy(B->graph); B->graph = nullptr; }
-    if (profit_threads) *profit_threads = bp;
-    if (combine_tile) *combine_tile = bt;
+    if (profit_threads) *profit_threads = pick.threads;
+    if (combine_tile) *combine_tile = pick.tile;
+    return BM_OK;
+}
+
+extern "C" bm_status bm_batch_set_schedule(bm_batch* B, int32_t persistent, int32_t profit_threads,
+                                           int32_t combine_tile) {
+    if (!B) return BM_E_INPUT;
+    if (combine_tile != 32 && combine_tile != 64) {
+        snprintf(B->err, sizeof B->err, "bm_batch_set_schedule: combine_tile %d is not 32 or 64", combine_tile);
+        return BM_E_INPUT;
+    }
+    if (persistent && !B->can_persist) {
+        snprintf(B->err, sizeof B->err, "bm_batch_set_schedule: no persistent schedule (largest instance %d > %d or "
+                 "the kernel does not fit)", B->max_n, kBSortMax);
+        return BM_E_INPUT;
+    }
+    if (!persistent && profit_threads != 256 && profit_threads != 512) {
+        snprintf(B->err, sizeof B->err, "bm_batch_set_schedule: profit_threads %d is not 256 or 512", profit_threads);
+        return BM_E_INPUT;
+    }
+    B->use_persist = persistent != 0;
+    B->profit_threads = persistent ? kBThreads : profit_threads;
+    B->tile = combine_tile;
+    bm_status s = batch_tiles(B);
+    if (s) return s;
+    if (B->exec) { cudaGraphExecDestroy(B->exec); B->exec = nullptr; }
+    if (B->graph) { cudaGraphDestroy(B->graph); B->graph = nullptr; }
     return BM_OK;
 }
 
@@ -557,7 +912,17 @@ extern "C" bm_status bm_batch_sweeps(bm_batch* B, int32_t sweeps, const bm_sweep
     std::vector<long long> dsum(B->count), csum(B->count);
     BK(cudaMemcpyAsync(dsum.data(), B->acc_delta, B->count * sizeof(long long), cudaMemcpyDeviceToHost, B->st));
     BK(cudaMemcpyAsync(csum.data(), B->acc_commits, B->count * sizeof(long long), cudaMemcpyDeviceToHost, B->st));
+    unsigned gerr = 0;
+    if (B->use_persist) BK(cudaMemcpyAsync(&gerr, B->gbar + 2, sizeof gerr, cudaMemcpyDeviceToHost, B->st));
     BK(cudaStreamSynchronize(B->st));
+    if (gerr) {
+        // a grid-barrier wait of the persistent sweep ran out: the matchings
+        // may be partly committed; the caller sets them again
+        BK(cudaMemset(B->gbar, 0, 4 * sizeof(unsigned)));
+        for (bm_ctx* c : B->ctx) { c->mapped = false; c->S_exact = false; }
+        snprintf(B->err, sizeof B->err, "bm_batch_sweeps: persistent sweep grid barrier wait timed out");
+        return BM_E_TIMEOUT;
+    }
     for (int i = 0; i < B->count; i++) {
         B->ctx[i]->score += dsum[i];
         if (committed) committed[i] = csum[i];

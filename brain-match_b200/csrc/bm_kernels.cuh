@@ -175,20 +175,24 @@ __device__ __forceinline__ void scatter_residual(int* acc, const typename Ent<W1
     }
 }
 
-// One profit row of S (all threads of the block call it together; it ends
-// with a barrier).  acc holds n+1 ints of shared memory.
+// One profit row of S by a group of threads that all call it together: the
+// whole block (NT = 0), or the NT threads (a power of two) of the block's
+// NT-aligned group; `sync` is a barrier over exactly those threads.  It ends
+// with a barrier.  acc holds n+1 ints of shared memory.
 // With `work`, the row also records its scheduling key for the next rebuild
 // (its scattered min terms + its edges + n if it has self-loops, the
 // estimate k_row_work makes) in work[a], and adds its terms to *work_total.
-template <bool W16>
-__device__ __forceinline__ void profit_row(const DevView<W16>& g, int a, int* acc, int2* s_long, int* s_nlong,
-                                           const unsigned char* __restrict__ is_hub, int hub_thr,
-                                           int* s_terms = nullptr, unsigned long long* work = nullptr,
-                                           unsigned long long* work_total = nullptr) {
+template <bool W16, int NT, typename Sync>
+__device__ __forceinline__ void profit_row_on(const DevView<W16>& g, int a, int* acc, int2* s_long, int* s_nlong,
+                                              const unsigned char* __restrict__ is_hub, int hub_thr, int* s_terms,
+                                              unsigned long long* work, unsigned long long* work_total, Sync sync) {
+    static_assert(NT == 0 || (NT & (NT - 1)) == 0, "group size is a power of two");
     typedef Ent<W16> EN;
     typedef typename EN::T E;
     const int n = g.n;
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+    const int tid = NT ? (int)(threadIdx.x & (NT - 1)) : (int)threadIdx.x;
+    const int nthr = NT ? NT : (int)blockDim.x;
+    const int lane = tid & 31, wid = tid >> 5, nw = nthr >> 5;
     if (tid == 0) {
         *s_nlong = 0;
         if (work) *s_terms = 0;
@@ -197,12 +201,12 @@ __device__ __forceinline__ void profit_row(const DevView<W16>& g, int a, int* ac
     // hub terms already in S are added when the row is written back
     if ((n & 3) == 0) {
         int4* a4 = reinterpret_cast<int4*>(acc);
-        for (int i = tid; i < (n >> 2); i += blockDim.x) a4[i] = make_int4(0, 0, 0, 0);
+        for (int i = tid; i < (n >> 2); i += nthr) a4[i] = make_int4(0, 0, 0, 0);
         if (tid == 0) acc[n] = 0;
     } else {
-        for (int i = tid; i <= n; i += blockDim.x) acc[i] = 0;
+        for (int i = tid; i <= n; i += nthr) acc[i] = 0;
     }
-    __syncthreads();
+    sync();
     // out-edges of a against G2 in-lists of p(v), then in-edges against out-lists of p(u)
     const int so = g.off1o[a], lo = g.off1o[a + 1] - so;
     const int si = g.off1i[a], li = g.off1i[a + 1] - si;
@@ -257,7 +261,7 @@ __device__ __forceinline__ void profit_row(const DevView<W16>& g, int a, int* ac
             scatter_list<W16>(acc, out ? g.ent2iP : g.ent2oP, b0t, b1t, w1t, lane, 32);
         }
     }
-    __syncthreads();
+    sync();
     // long lists, one at a time, by the whole block
     const int nl = min(*s_nlong, kLongQueue);
     for (int q = 0; q < nl; q++) {
@@ -266,13 +270,13 @@ __device__ __forceinline__ void profit_row(const DevView<W16>& g, int a, int* ac
         const int w1 = e.y & 0x7fffffff;
         const int* off = out ? g.off2i : g.off2o;
         const E* list = out ? g.ent2iP : g.ent2oP;
-        scatter_list<W16>(acc, list, off[e.x], off[e.x + 1], w1, tid, blockDim.x);
+        scatter_list<W16>(acc, list, off[e.x], off[e.x + 1], w1, tid, nthr);
     }
     // corner corrections for every G1 edge a->b
     {
         const int pa = g.p[a];
         const int dpa = g.w2d(pa);
-        for (int j = tid; j < lo; j += blockDim.x) {
+        for (int j = tid; j < lo; j += nthr) {
             const int b = EN::id(g.ent1o[so + j]);
             const E ep = g.ent1oP[so + j];
             const int pb = EN::id(ep), x = EN::w(ep);
@@ -285,8 +289,8 @@ __device__ __forceinline__ void profit_row(const DevView<W16>& g, int a, int* ac
     {
         const int q0 = g.offs[a], q1 = g.offs[a + 1];
         if (q1 > q0) {
-            __syncthreads();
-            for (int b = tid; b < n; b += blockDim.x) {
+            sync();
+            for (int b = tid; b < n; b += nthr) {
                 const int pb = g.p[b];
                 const int d = g.w2d(pb);
                 int t = 0;
@@ -295,7 +299,7 @@ __device__ __forceinline__ void profit_row(const DevView<W16>& g, int a, int* ac
             }
         }
     }
-    __syncthreads();
+    sync();
     if (work && tid == 0) {
         const long long terms = *s_terms;
         atomicAdd(work_total, (unsigned long long)terms);
@@ -309,32 +313,43 @@ __device__ __forceinline__ void profit_row(const DevView<W16>& g, int a, int* ac
         if (is_hub) {
             const int n4 = n >> 2;
             int i = tid;
-            for (; i + 3 * (int)blockDim.x < n4; i += 4 * blockDim.x) {
+            for (; i + 3 * (int)nthr < n4; i += 4 * nthr) {
                 int4 h[4];
 #pragma unroll
-                for (int u = 0; u < 4; u++) h[u] = r4[i + u * blockDim.x];
+                for (int u = 0; u < 4; u++) h[u] = r4[i + u * nthr];
 #pragma unroll
                 for (int u = 0; u < 4; u++) {
-                    const int4 v = a4[i + u * blockDim.x];
-                    r4[i + u * blockDim.x] = make_int4(h[u].x + v.x, h[u].y + v.y, h[u].z + v.z, h[u].w + v.w);
+                    const int4 v = a4[i + u * nthr];
+                    r4[i + u * nthr] = make_int4(h[u].x + v.x, h[u].y + v.y, h[u].z + v.z, h[u].w + v.w);
                 }
             }
-            for (; i < n4; i += blockDim.x) {
+            for (; i < n4; i += nthr) {
                 const int4 h = r4[i], v = a4[i];
                 r4[i] = make_int4(h.x + v.x, h.y + v.y, h.z + v.z, h.w + v.w);
             }
         } else {
-            for (int i = tid; i < (n >> 2); i += blockDim.x) r4[i] = a4[i];
+            for (int i = tid; i < (n >> 2); i += nthr) r4[i] = a4[i];
         }
     } else {
-        if (is_hub) for (int i = tid; i < n; i += blockDim.x) row[i] += acc[i];
-        else for (int i = tid; i < n; i += blockDim.x) row[i] = acc[i];
+        if (is_hub) for (int i = tid; i < n; i += nthr) row[i] += acc[i];
+        else for (int i = tid; i < n; i += nthr) row[i] = acc[i];
     }
-    __syncthreads();
+    sync();
+}
+
+// One profit row of S by the whole block (all threads call it together; it
+// ends with a barrier).
+template <bool W16>
+__device__ __forceinline__ void profit_row(const DevView<W16>& g, int a, int* acc, int2* s_long, int* s_nlong,
+                                           const unsigned char* __restrict__ is_hub, int hub_thr,
+                                           int* s_terms = nullptr, unsigned long long* work = nullptr,
+                                           unsigned long long* work_total = nullptr) {
+    profit_row_on<W16, 0>(g, a, acc, s_long, s_nlong, is_hub, hub_thr, s_terms, work, work_total,
+                          [] { __syncthreads(); });
 }
 
 template <bool W16>
-__global__ void __launch_bounds__(512)
+__global__ void __launch_bounds__(512, 3)
 k_profit(DevView<W16> g, const int* __restrict__ order, int* __restrict__ counter,
          const unsigned char* __restrict__ is_hub, int hub_thr, unsigned long long* __restrict__ work,
          unsigned long long* __restrict__ work_total) {

@@ -18,16 +18,23 @@ namespace bm {
 constexpr int kTile = 64;
 
 // One TxT tile (ti <= tj) of the upper triangle, 256 threads (T = 32 or 64).
-template <int T>
-__device__ __forceinline__ void combine_tile(const int* __restrict__ S, int n, int ti, int tj,
-                                             unsigned long long* __restrict__ part, int* __restrict__ all_out) {
+// Shared memory of one combine tile pass.
+template <int T> struct CombineSmem {
+    int sA[T][T + 1];               // sA[r][c] = S[a0+r][b0+c]
+    int sB[T][T + 1];               // sB[r][c] = S[b0+r][a0+c]
+    int dA[T], dB[T];
+    unsigned long long cpart[8][T];
+};
+
+// One tile pair by 256 threads (tid 0..255 among them; `sync` is a barrier
+// over exactly those threads), staged in `sm`.
+template <int T, typename Sync>
+__device__ __forceinline__ void combine_tile_on(const int* __restrict__ S, int n, int ti, int tj,
+                                                unsigned long long* __restrict__ part, int* __restrict__ all_out,
+                                                CombineSmem<T>& sm, int tid, Sync sync) {
     constexpr int CL = T / 32;            // columns per lane
-    __shared__ int sA[T][T + 1];          // sA[r][c] = S[a0+r][b0+c]
-    __shared__ int sB[T][T + 1];          // sB[r][c] = S[b0+r][a0+c]
-    __shared__ int dA[T], dB[T];
-    __shared__ unsigned long long cpart[8][T];
     const int a0 = ti * T, b0 = tj * T;
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;  // 8 warps
+    const int lane = tid & 31, wid = tid >> 5;  // 8 warps
     if ((n & 3) == 0) {
         // 16-byte streaming loads: with n a multiple of 4 every 4-column group
         // of a row is aligned and lies wholly inside or outside the matrix
@@ -38,24 +45,24 @@ __device__ __forceinline__ void combine_tile(const int* __restrict__ S, int n, i
             int4 va = make_int4(0, 0, 0, 0), vb = make_int4(0, 0, 0, 0);
             if (a < n && b < n) va = __ldcs(reinterpret_cast<const int4*>(S + (size_t)a * n + b));
             if (bb < n && aa < n) vb = __ldcs(reinterpret_cast<const int4*>(S + (size_t)bb * n + aa));
-            sA[r][c] = va.x; sA[r][c + 1] = va.y; sA[r][c + 2] = va.z; sA[r][c + 3] = va.w;
-            sB[r][c] = vb.x; sB[r][c + 1] = vb.y; sB[r][c + 2] = vb.z; sB[r][c + 3] = vb.w;
+            sm.sA[r][c] = va.x; sm.sA[r][c + 1] = va.y; sm.sA[r][c + 2] = va.z; sm.sA[r][c + 3] = va.w;
+            sm.sB[r][c] = vb.x; sm.sB[r][c + 1] = vb.y; sm.sB[r][c + 2] = vb.z; sm.sB[r][c + 3] = vb.w;
         }
     } else {
         for (int i = tid; i < T * T; i += 256) {
             const int r = i / T, c = i % T;
             const int a = a0 + r, b = b0 + c;
-            sA[r][c] = (a < n && b < n) ? S[(size_t)a * n + b] : 0;
+            sm.sA[r][c] = (a < n && b < n) ? S[(size_t)a * n + b] : 0;
             const int bb = b0 + r, aa = a0 + c;
-            sB[r][c] = (bb < n && aa < n) ? S[(size_t)bb * n + aa] : 0;
+            sm.sB[r][c] = (bb < n && aa < n) ? S[(size_t)bb * n + aa] : 0;
         }
     }
     if (tid < T) {
         const int a = a0 + tid, b = b0 + tid;
-        dA[tid] = a < n ? S[(size_t)a * n + a] : 0;
-        dB[tid] = b < n ? S[(size_t)b * n + b] : 0;
+        sm.dA[tid] = a < n ? S[(size_t)a * n + a] : 0;
+        sm.dB[tid] = b < n ? S[(size_t)b * n + b] : 0;
     }
-    __syncthreads();
+    sync();
     const bool diag = (ti == tj);
     // bests as 32-bit (delta, partner) pairs -- larger delta, then smaller
     // partner -- packed into the 64-bit key only for the reductions
@@ -70,7 +77,7 @@ __device__ __forceinline__ void combine_tile(const int* __restrict__ S, int n, i
             for (int q = 0; q < CL; q++) {
                 const int c = lane + 32 * q, b = b0 + c;
                 if (b < n && b != a) {
-                    const int d = sA[r][c] + sB[c][r] - dA[r] - dB[c];
+                    const int d = sm.sA[r][c] + sm.sB[c][r] - sm.dA[r] - sm.dB[c];
                     if (d > rd || (d == rd && b < ri)) { rd = d; ri = b; }
                     if (d > cbd[q] || (d == cbd[q] && a < cbi[q])) { cbd[q] = d; cbi[q] = a; }
                     if (all_out && a < b) all_out[(long long)a * (2LL * n - a - 1) / 2 + (b - a - 1)] = d;
@@ -88,15 +95,23 @@ __device__ __forceinline__ void combine_tile(const int* __restrict__ S, int n, i
     // diagonal tile's row partials already cover both orders of every pair
     if (!diag) {
 #pragma unroll
-        for (int q = 0; q < CL; q++) cpart[wid][lane + 32 * q] = cb[q];
-        __syncthreads();
+        for (int q = 0; q < CL; q++) sm.cpart[wid][lane + 32 * q] = cb[q];
+        sync();
         if (tid < T) {
-            unsigned long long k = cpart[0][tid];
-            for (int w = 1; w < 8; w++) k = kmax(k, cpart[w][tid]);
+            unsigned long long k = sm.cpart[0][tid];
+            for (int w = 1; w < 8; w++) k = kmax(k, sm.cpart[w][tid]);
             const int b = b0 + tid;
             if (b < n) part[(size_t)ti * n + b] = k;
         }
     }
+}
+
+// One tile pair by a 256-thread block.
+template <int T>
+__device__ __forceinline__ void combine_tile(const int* __restrict__ S, int n, int ti, int tj,
+                                             unsigned long long* __restrict__ part, int* __restrict__ all_out) {
+    __shared__ CombineSmem<T> sm;
+    combine_tile_on<T>(S, n, ti, tj, part, all_out, sm, threadIdx.x, [] { __syncthreads(); });
 }
 
 static __global__ void __launch_bounds__(256)

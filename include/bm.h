@@ -396,10 +396,13 @@ bm_status bm_quad_round(bm_ctx* ctx, const bm_quad_opts* opts, bm_quad_stats* st
 /*
  * Many independent graph pairs of uneven size swept together: every
  * instance keeps the single-instance semantics (bm_create, bm_sweep), and a
- * batch sweep runs all of them in one set of launches -- one persistent
+ * batch sweep runs all of them together, captured once as a CUDA graph and
+ * replayed, in one of two schedules: one persistent cooperative launch that
+ * runs every phase of the sweep for every instance behind grid barriers
+ * (instances up to 8,192 vertices), or a launch sequence -- one persistent
  * profit-row launch over every (instance, row), one combine launch over
- * every (instance, tile), one commit launch with a CTA per instance --
- * captured once as a CUDA graph and replayed.  The reference runs
+ * every (instance, tile), one commit launch with a CTA per instance.  The
+ * reference runs
  * independent instances as separate processes (MPI replicas,
  * src/mpi-omp.c:76-122) each with the sweep of
  * src/graph-re-alignment-gpu.cu:845-891.  The tensor-core hub term is not
@@ -420,14 +423,25 @@ bm_status bm_batch_set_mappings(bm_batch* b, const int32_t* const* maps);
 bm_status bm_batch_get_mappings(bm_batch* b, int32_t* const* maps);
 bm_status bm_batch_scores(bm_batch* b, int64_t* scores);
 /*
- * Times the candidate launch shapes (profit-row block 256/512 threads x
- * combine tile 32/64) on the batch itself and keeps the fastest; results
- * never depend on the choice.
+ * Times the candidate schedules on whole sweeps of the batch itself (the
+ * second and third sweep from the current matchings, which it restores) and
+ * keeps the fastest: the persistent
+ * launch (reported as profit_threads = 1024) with combine tile 32 or 64, and
+ * the launch sequence with profit-row blocks of 256 or 512 threads and tile
+ * 32 or 64.  Results never depend on the choice.
  */
 bm_status bm_batch_autotune(bm_batch* b, int32_t* profit_threads, int32_t* combine_tile);
 /*
+ * Sets the schedule directly: persistent != 0 for the one-launch sweep
+ * (BM_E_INPUT if the batch's largest instance exceeds 8,192 vertices), else
+ * the launch sequence with profit_threads 256 or 512; combine_tile 32 or 64.
+ */
+bm_status bm_batch_set_schedule(bm_batch* b, int32_t persistent, int32_t profit_threads, int32_t combine_tile);
+/*
  * Runs `sweeps` sweeps of every instance (graph replays).  committed (may be
  * NULL) receives per-instance swap counts; *ms the device time.
+ * BM_E_TIMEOUT if a grid-barrier wait of the persistent schedule ran out
+ * (the matchings must then be set again).
  */
 bm_status bm_batch_sweeps(bm_batch* b, int32_t sweeps, const bm_sweep_opts* opts, int64_t* committed,
                           float* ms);
