@@ -391,6 +391,18 @@ def run_batch(args, world, rank, local, pg):
     B = bm.Batch(pairs)
     info = B.info()
     B.set_mappings([g["map0"] for g in pairs])
+    schedules = None
+    if args.batch_schedules:
+        # every schedule set directly: sweeps 3-5 from the same random start, device ms per sweep
+        schedules = {}
+        for sched in ((True, 1024, 64), (True, 1024, 32), (False, 256, 64), (False, 256, 32), (False, 512, 64)):
+            B.set_mappings([g["map0"] for g in pairs])
+            B.set_schedule(*sched)
+            B.sweeps(2)
+            _, ms3 = B.sweeps(3)
+            name = ("persistent" if sched[0] else "sequence/%d" % sched[1]) + "/tile%d" % sched[2]
+            schedules[name] = ms3 / 3
+        B.set_mappings([g["map0"] for g in pairs])
     pt, tile = B.autotune()
     persistent = pt == 1024   # the one-launch schedule reports its 1024-thread CTA
     B.sweeps(args.warmup)
@@ -430,6 +442,7 @@ def run_batch(args, world, rank, local, pg):
             "e2e": {"value": world * args.steps * info["total_pairs"] / e2e_s, "unit": "deltas/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d // 2},
             "committed_last_steps": int(commits.sum()),
+            "schedules_ms_per_sweep": schedules,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
         }
@@ -954,6 +967,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-descent", action="store_true", help="skip the time-to-convergence descents")
+    ap.add_argument("--batch-schedules", action="store_true",
+                    help="batch64: also time every batch schedule set directly (sweeps 3-5 from the random start)")
     args = ap.parse_args()
     world, rank, local, pg = dist_setup()
     if args.impl == "reference" and args.workload in ("batch64", "triples", "quads", "greedy", "lookup",

@@ -17,7 +17,8 @@ BM_OK, BM_E_INPUT, BM_E_CUDA, BM_E_OVERFLOW, BM_E_TIMEOUT, BM_E_NOMEM, BM_E_STAT
 BM_FLAG_FORCE_I32 = 1
 BM_FLAG_NO_HUB_GEMM = 2
 BM_STATIC_MAX_PAIRS = 65536
-BM_STALL_HUB_GEMM, BM_STALL_COMMIT, BM_STALL_COMBINE, BM_STALL_GREEDY, BM_STALL_MLP_GEMM = 1, 2, 3, 4, 5
+BM_STALL_HUB_GEMM, BM_STALL_COMMIT, BM_STALL_COMBINE, BM_STALL_GREEDY, BM_STALL_MLP_GEMM, BM_STALL_BATCH = (
+    1, 2, 3, 4, 5, 6)
 
 
 class GenParams(C.Structure):

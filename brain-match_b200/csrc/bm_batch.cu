@@ -199,15 +199,13 @@ k_b_commit(const DevView<W16>* __restrict__ views, const BatchInst* __restrict__
 
 // ---------------------------------------------------------------------------
 // One batch sweep as one persistent launch: a cooperative grid of one
-// 1024-thread CTA per SM runs the phases above back to back, separated by a
-// bounded grid barrier:
-//   relabel -> profit rows (four 256-thread groups per CTA, an (instance,
-//   row) item each from a global counter) -> combine (four groups, an
-//   (instance, tile) item each) -> reduce ->
-//   candidates -> per instance (a CTA each): block radix sort of its
-//   candidate keys in shared memory, then the set commit.
-// Every phase's shared memory is the same dynamic buffer.  Row order does not
-// matter for the result (integer sums), so rows are taken in index order.
+// 1024-thread CTA per SM.  The relabel of every list of every instance comes
+// first, behind one bounded grid barrier; then a dataflow over the instances
+// (no further grid barrier, see the kernel): four 256-thread groups per CTA
+// take profit rows and combine tile pairs from one task counter, and each
+// instance's row bests, candidates, in-kernel candidate sort and set commit
+// run on the CTA that owns it as soon as its own tile pairs are done.  Row
+// order does not matter for the result (integer sums).
 constexpr int kBThreads = 1024;
 constexpr int kBSortItems = 8;                           // candidate keys per thread
 constexpr int kBSortMax = kBThreads * kBSortItems;       // instances up to 8,192 vertices
@@ -218,16 +216,19 @@ template <bool W16>
 struct BSweepArgs {
     const DevView<W16>* views;
     const BatchInst* inst;
-    const int* row_base;
-    const long long* tile_base;
     const long long* ebase;   // 4 count + 1: list segments laid end to end
     const typename Ent<W16>::T* const* lists;
-    int nb, total;
-    long long total_tiles;
-    int acc_w;             // ints per row accumulator (max n + 1, rounded up to 4)
-    int* counter;          // profit-row items taken
+    int nb;
+    const int* iorder;     // instances, largest first: the order of their tasks
+    const long long* tbase;   // 2 (count + 1): first row task, then first tile-pair task (from the
+                              // first tile-pair task) of each instance in that order
+    int total_tasks;       // every instance's rows and tile pairs
+    size_t group_bytes;    // shared memory of one 256-thread group (a row accumulator or a tile stage)
+    int* counter;          // tasks taken
+    int* done;             // 2 count: rows and tile pairs finished, per instance
     unsigned* bar;         // grid barrier: arrivals, generation, error
     int max_scan, max_verify;
+    int stall;             // test hook: the first grid barrier never completes
     CommitStats* st;
     long long* acc_delta;
     long long* acc_commits;
@@ -241,22 +242,25 @@ __device__ __forceinline__ unsigned b_ld_acquire(const unsigned* p) {
 
 // Grid-wide barrier of the co-resident CTAs.  A wait that runs out sets the
 // error word (bar[2]); every CTA leaves at its next barrier.  Returns false
-// once the error word is set.
-__device__ bool b_grid_barrier(unsigned* bar) {
+// once the error word is set.  With `stall` (the bm_test_stall hook) CTA 0
+// does not arrive and every CTA polls only a few thousand times, so the
+// barrier never completes and every CTA leaves at it.
+__device__ bool b_grid_barrier(unsigned* bar, bool stall = false) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
         __threadfence();
         const unsigned gen = b_ld_acquire(&bar[1]);
-        if (atomicAdd(&bar[0], 1u) == gridDim.x - 1) {
+        const unsigned limit = stall ? (1u << 12) : kBSpinLimit;
+        if (!(stall && blockIdx.x == 0) && atomicAdd(&bar[0], 1u) == gridDim.x - 1) {
             atomicExch(&bar[0], 0u);
             __threadfence();
             atomicAdd(&bar[1], 1u);
         } else {
             unsigned it = 0;
             while (b_ld_acquire(&bar[1]) == gen) {
-                if (b_ld_acquire(&bar[2]) || ++it > kBSpinLimit) {
+                if (b_ld_acquire(&bar[2]) || ++it > limit) {
                     atomicExch(&bar[2], 1u);
                     ok = 0;
                     break;
@@ -280,7 +284,6 @@ __global__ void __launch_bounds__(kBThreads, 1) k_b_sweep(BSweepArgs<W16> a) {
     typedef Ent<W16> EN;
     extern __shared__ __align__(16) unsigned char bsm[];
     const int tid = threadIdx.x;
-    const long long gt = (long long)blockIdx.x * blockDim.x + tid, gs = (long long)gridDim.x * blockDim.x;
     // relabel every instance's lists (G1 through p, G2 through pinv): the
     // lists laid end to end (segment 4b + lst starts at ebase[4b + lst]), each
     // CTA one contiguous range of that
@@ -302,103 +305,145 @@ __global__ void __launch_bounds__(kBThreads, 1) k_b_sweep(BSweepArgs<W16> a) {
             }
         }
     }
-    if (blockIdx.x == 0 && tid == 0) *a.counter = 0;   // read only after the barrier
-    if (!b_grid_barrier(a.bar)) return;
-    // profit rows: four groups of 256 threads, each with its own row
-    // accumulator, take (instance, row) items one at a time
-    {
-        const int grp = tid >> 8, gtid = tid & 255;
-        int* acc = reinterpret_cast<int*>(bsm) + (size_t)grp * a.acc_w;
-        __shared__ int s_item[4], s_nlong[4];
-        __shared__ int2 s_long[4][kLongQueue];
+    // the dataflow's counters start from zero (read only after the barrier)
+    if (blockIdx.x == 0) {
+        if (tid == 0) *a.counter = 0;
+        for (int i = tid; i < 2 * a.nb; i += blockDim.x) a.done[i] = 0;
+    }
+    if (!b_grid_barrier(a.bar, a.stall != 0)) return;
+    // Dataflow over the instances, with no further grid barrier: the tasks are
+    // every instance's rows, then every instance's tile pairs, each part with
+    // the largest instance first (iorder), and the four 256-thread groups of
+    // every CTA take them one at a time from a global counter.  A tile pair of
+    // instance i waits until all of i's rows are written (they were taken
+    // long before); the CTA that owns i (CTA i mod grid) stops taking tasks
+    // once all of i's tile pairs are done and runs i's row bests, candidates,
+    // candidate sort and set commit with all its threads -- so the largest
+    // instances' commits overlap the other instances' tile pairs.
+    // Dependencies point only to earlier tasks, which the groups that took
+    // them finish without waiting on later ones.
+    int* rows_done = a.done;
+    int* tiles_done = a.done + a.nb;
+    const int grp = tid >> 8, gtid = tid & 255;
+    unsigned char* gsm = bsm + (size_t)grp * a.group_bytes;     // the group's row accumulator or tile stage
+    int* acc = reinterpret_cast<int*>(gsm);
+    CombineSmem<T>& cs = *reinterpret_cast<CombineSmem<T>*>(gsm);
+    __shared__ int s_task[4], s_go[4];
+    __shared__ int s_nlong[4];
+    __shared__ int2 s_long[4][kLongQueue];
+    __shared__ int s_stop;
+    for (int own = blockIdx.x;; own += gridDim.x) {
+        const int target = own < a.nb ? a.inst[own].tiles * (a.inst[own].tiles + 1) / 2 : 0;
         for (;;) {
-            if (gtid == 0) s_item[grp] = atomicAdd(a.counter, 1);
+            if (gtid == 0) {
+                int go = !b_ld_acquire(&a.bar[2]);
+                if (go && own < a.nb && (int)b_ld_acquire((const unsigned*)&tiles_done[own]) >= target) go = 0;
+                int t = -1;
+                if (go && (t = atomicAdd(a.counter, 1)) >= a.total_tasks) go = 0;
+                s_task[grp] = t;
+                s_go[grp] = go;
+            }
             b_group_sync(grp);
-            const int r = s_item[grp];
-            if (r >= a.total) break;
-            const int b = find_inst(a.row_base, a.nb, r);
-            const DevView<W16> g = a.views[b];
-            profit_row_on<W16, 256>(g, r - a.row_base[b], acc, s_long[grp], &s_nlong[grp], nullptr, 0, nullptr,
-                                    nullptr, nullptr, [grp] { b_group_sync(grp); });
+            if (!s_go[grp]) break;
+            const int t = s_task[grp];
+            const bool row = t < a.tbase[a.nb];
+            const long long* base = row ? a.tbase : a.tbase + a.nb + 1;
+            const int k = find_inst_ll(base, a.nb, row ? t : t - a.tbase[a.nb]);
+            const int i = a.iorder[k];
+            const BatchInst I = a.inst[i];
+            const int local = (row ? t : t - (int)a.tbase[a.nb]) - (int)base[k] + (row ? 0 : I.n);
+            if (row) {           // profit row `local` of instance i
+                const DevView<W16> g = a.views[i];
+                profit_row_on<W16, 256>(g, local, acc, s_long[grp], &s_nlong[grp], nullptr, 0, nullptr, nullptr,
+                                        nullptr, [grp] { b_group_sync(grp); });
+                __threadfence();     // every thread's part of the row is visible before it counts
+                b_group_sync(grp);
+                if (gtid == 0) atomicAdd(&rows_done[i], 1);
+            } else {             // tile pair of instance i, once its rows are written
+                if (gtid == 0) {
+                    unsigned it = 0;
+                    while ((int)b_ld_acquire((const unsigned*)&rows_done[i]) < I.n) {
+                        if (b_ld_acquire(&a.bar[2]) || ++it > kBSpinLimit) { atomicExch(&a.bar[2], 1u); break; }
+                        __nanosleep(64);
+                    }
+                    __threadfence();
+                }
+                b_group_sync(grp);
+                long long q = local - I.n;
+                int ti = 0;
+                while (q >= I.tiles - ti) { q -= I.tiles - ti; ti++; }
+                const int tj = ti + (int)q;
+                combine_tile_on<T>(I.S, I.n, ti, tj, I.part, nullptr, cs, gtid, [grp] { b_group_sync(grp); });
+                __threadfence();     // the tile's partial bests are visible before it counts
+                b_group_sync(grp);   // (and cs is rewritten by the group's next task)
+                if (gtid == 0) atomicAdd(&tiles_done[i], 1);
+            }
         }
-    }
-    if (!b_grid_barrier(a.bar)) return;
-    // combine: four groups of 256 threads, an (instance, tile) item each
-    {
-        const int grp = tid >> 8, gtid = tid & 255;
-        CombineSmem<T>& cs = reinterpret_cast<CombineSmem<T>*>(bsm)[grp];
-        for (long long it = (long long)blockIdx.x * 4 + grp; it < a.total_tiles; it += 4LL * gridDim.x) {
-            const int b = find_inst_ll(a.tile_base, a.nb, it);
-            const BatchInst I = a.inst[b];
-            long long t = it - a.tile_base[b];
-            int ti = 0;
-            while (t >= I.tiles - ti) { t -= I.tiles - ti; ti++; }
-            const int tj = ti + (int)t;
-            combine_tile_on<T>(I.S, I.n, ti, tj, I.part, nullptr, cs, gtid, [grp] { b_group_sync(grp); });
-            b_group_sync(grp);   // cs is rewritten by the group's next item
+        __syncthreads();   // all four groups have stopped
+        if (own >= a.nb) break;
+        // ---- instance `own`: wait for its tile pairs, then its bests, candidates, sort and commit
+        if (tid == 0) {
+            unsigned it = 0;
+            while ((int)b_ld_acquire((const unsigned*)&tiles_done[own]) < target) {
+                if (b_ld_acquire(&a.bar[2]) || ++it > kBSpinLimit) { atomicExch(&a.bar[2], 1u); break; }
+                __nanosleep(64);
+            }
+            __threadfence();
+            s_stop = b_ld_acquire(&a.bar[2]) != 0;
         }
-    }
-    if (!b_grid_barrier(a.bar)) return;
-    // row bests: max over the tile partials
-    for (long long x = gt; x < a.total; x += gs) {
-        const int b = find_inst(a.row_base, a.nb, (int)x);
-        const BatchInst I = a.inst[b];
-        const int xi = (int)x - a.row_base[b];
-        unsigned long long k = 0;
-        for (int t = 0; t < I.tiles; t++) k = kmax(k, I.part[(size_t)t * I.n + xi]);
-        I.rowbest[xi] = k;
-    }
-    if (!b_grid_barrier(a.bar)) return;
-    // candidate keys (the single-instance rule, k_candidates)
-    for (long long x = gt; x < a.total; x += gs) {
-        const int b = find_inst(a.row_base, a.nb, (int)x);
-        const BatchInst I = a.inst[b];
-        const int xa = (int)x - a.row_base[b];
-        const unsigned long long k = I.rowbest[xa];
-        unsigned long long out = ~0ull;
-        if (k) {
-            const int d = (int)((unsigned)(k >> 32) - 0x80000000u);
-            const int q = (int)(~(unsigned)(k & 0xffffffffu));
-            if (d > 0) {
-                const unsigned long long kb = I.rowbest[q];
-                const int qq = (int)(~(unsigned)(kb & 0xffffffffu));
-                const bool mutual = (kb != 0) && (qq == xa);
-                if (!mutual || xa < q) {
-                    const int lo = xa < q ? xa : q, hi = xa < q ? q : xa;
-                    out = ((unsigned long long)(0x7fffffffu - (unsigned)d) << 32) |
-                          ((unsigned long long)lo << 16) | (unsigned long long)hi;
+        __syncthreads();
+        if (s_stop) break;
+        const BatchInst I = a.inst[own];
+        for (int x = tid; x < I.n; x += blockDim.x) {
+            unsigned long long k = 0;
+            for (int tt = 0; tt < I.tiles; tt++) k = kmax(k, __ldcg(&I.part[(size_t)tt * I.n + x]));
+            I.rowbest[x] = k;
+        }
+        __syncthreads();
+        // candidate keys (the single-instance rule, k_candidates)
+        for (int xa = tid; xa < I.n; xa += blockDim.x) {
+            const unsigned long long k = I.rowbest[xa];
+            unsigned long long out = ~0ull;
+            if (k) {
+                const int d = (int)((unsigned)(k >> 32) - 0x80000000u);
+                const int q = (int)(~(unsigned)(k & 0xffffffffu));
+                if (d > 0) {
+                    const unsigned long long kb = I.rowbest[q];
+                    const int qq = (int)(~(unsigned)(kb & 0xffffffffu));
+                    const bool mutual = (kb != 0) && (qq == xa);
+                    if (!mutual || xa < q) {
+                        const int lo = xa < q ? xa : q, hi = xa < q ? q : xa;
+                        out = ((unsigned long long)(0x7fffffffu - (unsigned)d) << 32) |
+                              ((unsigned long long)lo << 16) | (unsigned long long)hi;
+                    }
                 }
             }
+            I.keys[xa] = out;
         }
-        I.keys[xa] = out;
-    }
-    if (!b_grid_barrier(a.bar)) return;
-    // per instance: sort its candidates in shared memory, then the set commit
-    for (int b = blockIdx.x; b < a.nb; b += gridDim.x) {
-        const BatchInst I = a.inst[b];
-        {
+        __syncthreads();
+        {   // sort the candidate keys in shared memory
             typename BSort::TempStorage& ts = *reinterpret_cast<typename BSort::TempStorage*>(bsm);
-            unsigned long long k[kBSortItems];
+            unsigned long long kk[kBSortItems];
 #pragma unroll
             for (int q = 0; q < kBSortItems; q++) {
-                const int i = tid * kBSortItems + q;
-                k[q] = i < I.n ? I.keys[i] : ~0ull;
+                const int x = tid * kBSortItems + q;
+                kk[q] = x < I.n ? I.keys[x] : ~0ull;
             }
-            BSort(ts).Sort(k);
+            BSort(ts).Sort(kk);
 #pragma unroll
             for (int q = 0; q < kBSortItems; q++) {
-                const int i = tid * kBSortItems + q;
-                if (i < I.n) I.keys_sorted[i] = k[q];
+                const int x = tid * kBSortItems + q;
+                if (x < I.n) I.keys_sorted[x] = kk[q];
             }
         }
         __syncthreads();
-        const DevView<W16> g = a.views[b];
+        const DevView<W16> g = a.views[own];
         const int lim = (a.max_scan > 0 && a.max_scan < I.n) ? a.max_scan : I.n;
-        commit_group<W16, kCGBatch>(g, I.keys_sorted, lim, a.max_verify, &a.st[b], bsm);
+        commit_group<W16, kCGBatch>(g, I.keys_sorted, lim, a.max_verify, &a.st[own], bsm);
         __syncthreads();
         if (tid == 0) {
-            a.acc_delta[b] += a.st[b].total_delta;
-            a.acc_commits[b] += a.st[b].committed;
+            a.acc_delta[own] += a.st[own].total_delta;
+            a.acc_commits[own] += a.st[own].committed;
         }
         __syncthreads();
     }
@@ -422,6 +467,13 @@ struct bm_batch {
     long long* tile_base = nullptr;       // count+1
     long long *e1 = nullptr, *e2 = nullptr;
     long long* ebase = nullptr;           // 4 count + 1: the lists laid end to end (persistent relabel)
+    // the persistent schedule's dataflow: instances largest first, the first
+    // row task and tile-pair task of each in that order, per-instance
+    // finished rows and tile pairs
+    int* iorder = nullptr;
+    long long* tbase = nullptr;
+    long long total_tasks = 0;
+    int* done = nullptr;
     void** lists = nullptr;               // 4 per instance: ent1o, ent1i, ent2o, ent2i
     unsigned long long *wkeys = nullptr, *wkeys_sorted = nullptr, *ckeys = nullptr, *ckeys_sorted = nullptr;
     int *wvals = nullptr, *order = nullptr;
@@ -466,7 +518,8 @@ static void batch_free(bm_batch* B) {
     if (B->graph) cudaGraphDestroy(B->graph);
     void* bufs[] = {B->views, B->inst, B->row_base, B->tile_base, B->e1, B->e2, B->lists, B->wkeys,
                     B->wkeys_sorted, B->ckeys, B->ckeys_sorted, B->wvals, B->order, B->rowbest, B->part,
-                    B->cub_tmp, B->counter, B->cstats, B->acc_delta, B->acc_commits, B->gbar, B->ebase};
+                    B->cub_tmp, B->counter, B->cstats, B->acc_delta, B->acc_commits, B->gbar, B->ebase,
+                    B->iorder, B->tbase, B->done};
     for (void* p : bufs) if (p) cudaFree(p);
     if (B->ev0) cudaEventDestroy(B->ev0);
     if (B->ev1) cudaEventDestroy(B->ev1);
@@ -489,6 +542,22 @@ static bm_status batch_tiles(bm_batch* B) {
     }
     B->total_tiles = tb[B->count];
     BK(cudaMemcpy(B->tile_base, tb.data(), tb.size() * sizeof(long long), cudaMemcpyHostToDevice));
+    if (B->iorder) {   // the persistent schedule's task layout: per instance, largest first, rows then tile pairs
+        std::vector<int> ord(B->count);
+        for (int i = 0; i < B->count; i++) ord[i] = i;
+        std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return B->hinst[x].n > B->hinst[y].n; });
+        // [rows prefix (count + 1)][tile-pair prefix (count + 1)]
+        std::vector<long long> tbase(2 * (size_t)B->count + 2, 0);
+        for (int k = 0; k < B->count; k++) {
+            const BatchInst& I = B->hinst[ord[k]];
+            tbase[k + 1] = tbase[k] + I.n;
+            tbase[B->count + 1 + k + 1] = tbase[B->count + 1 + k] + (long long)I.tiles * (I.tiles + 1) / 2;
+        }
+        B->total_tasks = tbase[B->count] + tbase[2 * (size_t)B->count + 1];
+        if (B->total_tasks > 0x7fffffffLL) B->can_persist = B->use_persist = false;   // 32-bit task indices
+        BK(cudaMemcpy(B->iorder, ord.data(), ord.size() * sizeof(int), cudaMemcpyHostToDevice));
+        BK(cudaMemcpy(B->tbase, tbase.data(), tbase.size() * sizeof(long long), cudaMemcpyHostToDevice));
+    }
     BK(cudaMemcpy(B->inst, B->hinst.data(), B->hinst.size() * sizeof(BatchInst), cudaMemcpyHostToDevice));
     return BM_OK;
 }
@@ -618,6 +687,9 @@ extern "C" bm_status bm_batch_create(bm_batch** out, int32_t count, const int32_
         if (s2) return s2;
         BK(cudaMalloc(&B->gbar, 4 * sizeof(unsigned)));
         BK(cudaMemset(B->gbar, 0, 4 * sizeof(unsigned)));
+        BK(cudaMalloc(&B->iorder, count * sizeof(int)));
+        BK(cudaMalloc(&B->tbase, 2 * (count + 1) * sizeof(long long)));
+        BK(cudaMalloc(&B->done, 2 * count * sizeof(int)));
         s2 = B->w16 ? persistent_setup<true>(B) : persistent_setup<false>(B);
         if (s2) return s2;
         return batch_tiles(B);
@@ -660,10 +732,17 @@ extern "C" bm_status bm_batch_scores(bm_batch* B, int64_t* scores) {
 }
 
 // Shared memory of k_b_sweep: the largest of its phases' needs.
+// Shared memory of one 256-thread group of k_b_sweep: a row accumulator or a
+// tile stage, whichever is larger.
+template <int T>
+static size_t persistent_group_bytes(int max_n) {
+    const size_t row = (size_t)((max_n + 1 + 3) & ~3) * sizeof(int);
+    return (std::max(row, sizeof(CombineSmem<T>)) + 15) & ~(size_t)15;
+}
+
 template <int T>
 static size_t persistent_smem(int max_n) {
-    size_t m = 4 * (size_t)((max_n + 1 + 3) & ~3) * sizeof(int);         // four profit rows
-    m = std::max(m, 4 * sizeof(CombineSmem<T>));                           // four combine groups
+    size_t m = 4 * persistent_group_bytes<T>(max_n);                      // four groups
     m = std::max(m, sizeof(typename BSort::TempStorage));                  // the candidate sort
     m = std::max(m, commit_group_smem(max_n));                             // the set commit
     return (m + 15) & ~(size_t)15;
@@ -698,22 +777,23 @@ static bm_status persistent_setup(bm_batch* B) {
 }
 
 template <bool W16>
-static bm_status enqueue_persistent(bm_batch* B, int max_scan, int max_verify) {
+static bm_status enqueue_persistent(bm_batch* B, int max_scan, int max_verify, int stall = 0) {
     BSweepArgs<W16> a;
     a.views = (const DevView<W16>*)B->views;
     a.inst = B->inst;
-    a.row_base = B->row_base;
-    a.tile_base = B->tile_base;
     a.ebase = B->ebase;
     a.lists = (const typename Ent<W16>::T* const*)B->lists;
     a.nb = B->count;
-    a.total = B->total;
-    a.total_tiles = B->total_tiles;
-    a.acc_w = (B->max_n + 1 + 3) & ~3;
+    a.iorder = B->iorder;
+    a.tbase = B->tbase;
+    a.total_tasks = (int)B->total_tasks;
+    a.group_bytes = B->tile == 32 ? persistent_group_bytes<32>(B->max_n) : persistent_group_bytes<64>(B->max_n);
     a.counter = B->counter;
+    a.done = B->done;
     a.bar = B->gbar;
     a.max_scan = max_scan;
     a.max_verify = max_verify;
+    a.stall = stall;
     a.st = B->cstats;
     a.acc_delta = B->acc_delta;
     a.acc_commits = B->acc_commits;
@@ -906,7 +986,16 @@ extern "C" bm_status bm_batch_sweeps(bm_batch* B, int32_t sweeps, const bm_sweep
     }
     BK(cudaMemsetAsync(B->acc_delta, 0, B->count * sizeof(long long), B->st));
     BK(cudaMemsetAsync(B->acc_commits, 0, B->count * sizeof(long long), B->st));
+    // test hook (bm_test_stall): one sweep launched outside the graph whose
+    // first grid barrier never completes
+    const int stall = (B->use_persist && sweeps > 0) ? take_stall(BM_STALL_BATCH) : 0;
     BK(cudaEventRecord(B->ev0, B->st));
+    if (stall) {
+        bm_status s = B->w16 ? enqueue_persistent<true>(B, max_scan, max_verify, 1)
+                             : enqueue_persistent<false>(B, max_scan, max_verify, 1);
+        if (s) return s;
+        sweeps = 0;
+    }
     for (int i = 0; i < sweeps; i++) BK(cudaGraphLaunch(B->exec, B->st));
     BK(cudaEventRecord(B->ev1, B->st));
     std::vector<long long> dsum(B->count), csum(B->count);

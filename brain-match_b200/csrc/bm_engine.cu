@@ -42,7 +42,7 @@ int take_stall(int site) {
 }
 
 extern "C" bm_status bm_test_stall(int32_t site) {
-    if (site < 0 || site > BM_STALL_MLP_GEMM) return BM_E_INPUT;
+    if (site < 0 || site > BM_STALL_BATCH) return BM_E_INPUT;
     g_stall.store(site);
     return BM_OK;
 }

@@ -268,6 +268,7 @@ bm_status bm_measure_peaks(int32_t n, double* red_per_s, double* minadd_per_s);
 #define BM_STALL_COMBINE    3   /* bm_sweep: TMA-fed pair combine          */
 #define BM_STALL_GREEDY     4   /* bm_greedy_match: grid barrier           */
 #define BM_STALL_MLP_GEMM   5   /* bm_mlp_*: tensor-core GEMM              */
+#define BM_STALL_BATCH      6   /* bm_batch_sweeps: persistent sweep grid barrier */
 bm_status bm_test_stall(int32_t site);
 
 /* ---- Exact swap-lookup table ----

@@ -73,6 +73,32 @@ def test_mlp_gemm_wait_runs_out():
     np.testing.assert_allclose(grads, grads2, rtol=1e-4, atol=1e-6)
 
 
+def test_batch_grid_barrier_wait_runs_out():
+    """The persistent batch sweep's grid barrier: the stalled sweep returns
+    BM_E_TIMEOUT, the matchings must be set again, and the batch then makes
+    every instance's own moves."""
+    pairs = [bm.generate(bm.gen_params(n=n, e=20 * n, seed=500 + i)) for i, n in enumerate((300, 700, 1100))]
+    with bm.Batch(pairs) as B:
+        B.set_schedule(True, 1024, 64)
+        B.set_mappings([g["map0"] for g in pairs])
+        bm.test_stall(bm.BM_STALL_BATCH)
+        with pytest.raises(bm.BMError) as e:
+            B.sweeps(2)
+        assert e.value.status == bm.BM_E_TIMEOUT and "grid barrier wait timed out" in str(e.value)
+        with pytest.raises(bm.BMError) as e:
+            B.sweeps(1)
+        assert e.value.status == bm.BM_E_STATE
+        B.set_mappings([g["map0"] for g in pairs])
+        B.sweeps(2)
+        maps = B.get_mappings()
+    for i, g in enumerate(pairs):
+        with bm.Engine.from_pair(g, bm.BM_FLAG_NO_HUB_GEMM) as E:
+            E.set_mapping(g["map0"])
+            E.sweep()
+            E.sweep()
+            assert np.array_equal(E.get_mapping(), maps[i]), i
+
+
 def test_stall_hook_rejects_unknown_sites():
     with pytest.raises(bm.BMError) as e:
         bm.test_stall(99)
