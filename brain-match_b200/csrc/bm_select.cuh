@@ -288,9 +288,14 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
     if (tid == 0) { s_n = 0; s_k = 0; s_scanned = 0; p16[n] = (uint16_t)n; }
     long long total = 0, entries = 0;
     int verified = 0, committed = 0, steps = 0;
-    int pf_base = -1;                  // warp 0: start of the window prefetched into s_pfkey, s_pfinf
-    __shared__ unsigned long long s_pfkey[32];
-    __shared__ int4 s_pfinf[32][2];
+    // warp 0: the next kPF candidates (keys and list extents), prefetched into
+    // shared memory at the end of each step; a step scans ~180 candidates early
+    // in a descent, so a 32-wide window left one L2 round trip per further 32
+    constexpr int kPF = 256;
+    int pf_base = -1;                  // warp 0: first candidate of the prefetched window
+    bool pf_waited = false;
+    __shared__ unsigned long long s_pfkey[kPF];
+    __shared__ int4 s_pfinf[kPF][2];
     __syncthreads();
     for (;;) {
         // ---- warp 0: the next live candidates, then the
@@ -301,9 +306,14 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
                 const int idx = k + lane;
                 unsigned long long key;
                 int4 i0 = make_int4(0, 0, 0, 0), i1 = make_int4(0, 0, 0, 0);
-                if (k == pf_base) {  // the window prefetched at the end of the last step
-                    asm volatile("cp.async.wait_group 0;" ::: "memory");
-                    key = s_pfkey[lane]; i0 = s_pfinf[lane][0]; i1 = s_pfinf[lane][1];
+                const int off = k - pf_base;
+                if (cinfo && pf_base >= 0 && off >= 0 && off + 32 <= kPF) {   // inside the prefetched window
+                    if (!pf_waited) {   // every lane's copies have landed (lanes read each other's slots)
+                        asm volatile("cp.async.wait_group 0;" ::: "memory");
+                        __syncwarp();
+                        pf_waited = true;
+                    }
+                    key = s_pfkey[off + lane]; i0 = s_pfinf[off + lane][0]; i1 = s_pfinf[off + lane][1];
                 } else {
                     key = idx < lim ? keys[idx] : ~0ull;
                     if (cinfo && idx < lim) { i0 = cinfo[2 * idx]; i1 = cinfo[2 * idx + 1]; }
@@ -343,19 +353,26 @@ __device__ __forceinline__ void commit_group(const DevView<W16>& g, const unsign
             }
             // prefetch the next window (its keys and list extents); it is used as
             // is, since only the used flags change and those are read at use
-            if (cinfo) {  // asynchronous copies straight into shared memory, each lane its own slot
-                const int idx = k + lane;
+            if (cinfo) {  // asynchronous copies straight into shared memory, lane l the slots l, l + 32, ...
+                if (!pf_waited && pf_base >= 0) {   // copies of a window never read must land first
+                    asm volatile("cp.async.wait_group 0;" ::: "memory");
+                }
+                __syncwarp();   // every lane is done reading the previous window
                 pf_base = k;
-                if (idx < lim) {
-                    const uint32_t dk = (uint32_t)__cvta_generic_to_shared(&s_pfkey[lane]);
-                    const uint32_t di = (uint32_t)__cvta_generic_to_shared(&s_pfinf[lane][0]);
-                    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" :: "r"(dk), "l"(keys + idx) : "memory");
-                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(di), "l"(cinfo + 2 * idx) : "memory");
-                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(di + 16), "l"(cinfo + 2 * idx + 1) : "memory");
-                } else {
-                    s_pfkey[lane] = ~0ull;
-                    s_pfinf[lane][0] = make_int4(0, 0, 0, 0);
-                    s_pfinf[lane][1] = make_int4(0, 0, 0, 0);
+                pf_waited = false;
+                for (int h = 0; h < kPF / 32; h++) {
+                    const int slot = 32 * h + lane, idx = k + slot;
+                    if (idx < lim) {
+                        const uint32_t dk = (uint32_t)__cvta_generic_to_shared(&s_pfkey[slot]);
+                        const uint32_t di = (uint32_t)__cvta_generic_to_shared(&s_pfinf[slot][0]);
+                        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" :: "r"(dk), "l"(keys + idx) : "memory");
+                        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(di), "l"(cinfo + 2 * idx) : "memory");
+                        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(di + 16), "l"(cinfo + 2 * idx + 1) : "memory");
+                    } else {
+                        s_pfkey[slot] = ~0ull;
+                        s_pfinf[slot][0] = make_int4(0, 0, 0, 0);
+                        s_pfinf[slot][1] = make_int4(0, 0, 0, 0);
+                    }
                 }
                 asm volatile("cp.async.commit_group;" ::: "memory");
             }
