@@ -220,6 +220,7 @@ struct BSweepArgs {
     const typename Ent<W16>::T* const* lists;
     int nb;
     const int* iorder;     // instances, largest first: the order of their tasks
+    const int* rpt;        // rows per row task: 2 when two of the instance's rows fit a group's shared memory
     const long long* tbase;   // 2 (count + 1): first row task, then first tile-pair task (from the
                               // first tile-pair task) of each instance in that order
     int total_tasks;       // every instance's rows and tile pairs
@@ -329,8 +330,8 @@ __global__ void __launch_bounds__(kBThreads, 1) k_b_sweep(BSweepArgs<W16> a) {
     int* acc = reinterpret_cast<int*>(gsm);
     CombineSmem<T>& cs = *reinterpret_cast<CombineSmem<T>*>(gsm);
     __shared__ int s_task[4], s_go[4];
-    __shared__ int s_nlong[4];
-    __shared__ int2 s_long[4][kLongQueue];
+    __shared__ int s_nlong[8];
+    __shared__ int2 s_long[8][kLongQueue];   // per group, or per half-group for paired rows
     __shared__ int s_stop;
     for (int own = blockIdx.x;; own += gridDim.x) {
         const int target = own < a.nb ? a.inst[own].tiles * (a.inst[own].tiles + 1) / 2 : 0;
@@ -352,13 +353,27 @@ __global__ void __launch_bounds__(kBThreads, 1) k_b_sweep(BSweepArgs<W16> a) {
             const int i = a.iorder[k];
             const BatchInst I = a.inst[i];
             const int local = (row ? t : t - (int)a.tbase[a.nb]) - (int)base[k] + (row ? 0 : I.n);
-            if (row) {           // profit row `local` of instance i
+            if (row) {
                 const DevView<W16> g = a.views[i];
-                profit_row_on<W16, 256>(g, local, acc, s_long[grp], &s_nlong[grp], nullptr, 0, nullptr, nullptr,
-                                        nullptr, [grp] { b_group_sync(grp); });
-                __threadfence();     // every thread's part of the row is visible before it counts
-                b_group_sync(grp);
-                if (gtid == 0) atomicAdd(&rows_done[i], 1);
+                if (a.rpt[i] == 1) {   // profit row `local` of instance i by the whole group
+                    // (the long-list queue of the group's first half: halves of other groups use theirs)
+                    profit_row_on<W16, 256>(g, local, acc, s_long[2 * grp], &s_nlong[2 * grp], nullptr, 0, nullptr,
+                                            nullptr, nullptr, [grp] { b_group_sync(grp); });
+                    __threadfence();     // every thread's part of the row is visible before it counts
+                    b_group_sync(grp);
+                    if (gtid == 0) atomicAdd(&rows_done[i], 1);
+                } else {               // rows 2 local and 2 local + 1, a 128-thread half and accumulator each
+                    const int half = gtid >> 7, r = 2 * local + half;
+                    const int hb = 2 * grp + half;   // the half's barrier: 5 + hb, 128 threads
+                    if (r < I.n)
+                        profit_row_on<W16, 128>(g, r, acc + half * ((I.n + 1 + 3) & ~3), s_long[hb], &s_nlong[hb],
+                                                nullptr, 0, nullptr, nullptr, nullptr, [hb] {
+                                                    asm volatile("bar.sync %0, 128;" :: "r"(5 + hb) : "memory");
+                                                });
+                    __threadfence();
+                    b_group_sync(grp);
+                    if (gtid == 0) atomicAdd(&rows_done[i], min(2, I.n - 2 * local));
+                }
             } else {             // tile pair of instance i, once its rows are written
                 if (gtid == 0) {
                     unsigned it = 0;
@@ -471,6 +486,7 @@ struct bm_batch {
     // row task and tile-pair task of each in that order, per-instance
     // finished rows and tile pairs
     int* iorder = nullptr;
+    int* rpt = nullptr;                   // rows per row task of each instance (1 or 2)
     long long* tbase = nullptr;
     long long total_tasks = 0;
     int* done = nullptr;
@@ -501,6 +517,8 @@ static thread_local char g_batch_create_err[512];
 
 template <bool W16>
 static bm_status persistent_setup(bm_batch* B);
+template <int T>
+static size_t persistent_group_bytes(int max_n);
 
 #define BK(call)                                                                         \
     do {                                                                                 \
@@ -519,7 +537,7 @@ static void batch_free(bm_batch* B) {
     void* bufs[] = {B->views, B->inst, B->row_base, B->tile_base, B->e1, B->e2, B->lists, B->wkeys,
                     B->wkeys_sorted, B->ckeys, B->ckeys_sorted, B->wvals, B->order, B->rowbest, B->part,
                     B->cub_tmp, B->counter, B->cstats, B->acc_delta, B->acc_commits, B->gbar, B->ebase,
-                    B->iorder, B->tbase, B->done};
+                    B->iorder, B->tbase, B->done, B->rpt};
     for (void* p : bufs) if (p) cudaFree(p);
     if (B->ev0) cudaEventDestroy(B->ev0);
     if (B->ev1) cudaEventDestroy(B->ev1);
@@ -546,16 +564,22 @@ static bm_status batch_tiles(bm_batch* B) {
         std::vector<int> ord(B->count);
         for (int i = 0; i < B->count; i++) ord[i] = i;
         std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return B->hinst[x].n > B->hinst[y].n; });
+        // two rows per row task where both accumulators fit a group's shared memory
+        const size_t gb = B->tile == 32 ? persistent_group_bytes<32>(B->max_n) : persistent_group_bytes<64>(B->max_n);
+        std::vector<int> rpt(B->count);
+        for (int i = 0; i < B->count; i++)
+            rpt[i] = 2 * (size_t)((B->hinst[i].n + 1 + 3) & ~3) * sizeof(int) <= gb ? 2 : 1;
         // [rows prefix (count + 1)][tile-pair prefix (count + 1)]
         std::vector<long long> tbase(2 * (size_t)B->count + 2, 0);
         for (int k = 0; k < B->count; k++) {
             const BatchInst& I = B->hinst[ord[k]];
-            tbase[k + 1] = tbase[k] + I.n;
+            tbase[k + 1] = tbase[k] + (I.n + rpt[ord[k]] - 1) / rpt[ord[k]];
             tbase[B->count + 1 + k + 1] = tbase[B->count + 1 + k] + (long long)I.tiles * (I.tiles + 1) / 2;
         }
         B->total_tasks = tbase[B->count] + tbase[2 * (size_t)B->count + 1];
         if (B->total_tasks > 0x7fffffffLL) B->can_persist = B->use_persist = false;   // 32-bit task indices
         BK(cudaMemcpy(B->iorder, ord.data(), ord.size() * sizeof(int), cudaMemcpyHostToDevice));
+        BK(cudaMemcpy(B->rpt, rpt.data(), rpt.size() * sizeof(int), cudaMemcpyHostToDevice));
         BK(cudaMemcpy(B->tbase, tbase.data(), tbase.size() * sizeof(long long), cudaMemcpyHostToDevice));
     }
     BK(cudaMemcpy(B->inst, B->hinst.data(), B->hinst.size() * sizeof(BatchInst), cudaMemcpyHostToDevice));
@@ -688,6 +712,7 @@ extern "C" bm_status bm_batch_create(bm_batch** out, int32_t count, const int32_
         BK(cudaMalloc(&B->gbar, 4 * sizeof(unsigned)));
         BK(cudaMemset(B->gbar, 0, 4 * sizeof(unsigned)));
         BK(cudaMalloc(&B->iorder, count * sizeof(int)));
+        BK(cudaMalloc(&B->rpt, count * sizeof(int)));
         BK(cudaMalloc(&B->tbase, 2 * (count + 1) * sizeof(long long)));
         BK(cudaMalloc(&B->done, 2 * count * sizeof(int)));
         s2 = B->w16 ? persistent_setup<true>(B) : persistent_setup<false>(B);
@@ -785,6 +810,7 @@ static bm_status enqueue_persistent(bm_batch* B, int max_scan, int max_verify, i
     a.lists = (const typename Ent<W16>::T* const*)B->lists;
     a.nb = B->count;
     a.iorder = B->iorder;
+    a.rpt = B->rpt;
     a.tbase = B->tbase;
     a.total_tasks = (int)B->total_tasks;
     a.group_bytes = B->tile == 32 ? persistent_group_bytes<32>(B->max_n) : persistent_group_bytes<64>(B->max_n);

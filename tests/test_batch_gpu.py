@@ -58,8 +58,10 @@ def test_batch_mixed_weights_uses_one_storage_mode():
 @pytest.mark.parametrize("sched", [(True, 1024, 32), (True, 1024, 64), (False, 256, 32), (False, 512, 64)])
 def test_batch_schedules_match_single_instances(sched):
     """Each schedule, set directly, gives every instance the moves it makes
-    alone (the persistent launch also with 32-bit entries)."""
-    pairs = _pairs([300, 517, 800, 1203, 64, 2600], seed0=400)
+    alone (the persistent launch also with 32-bit entries).  The sizes mix
+    instances whose rows the persistent launch pairs on half groups with
+    larger ones it does not."""
+    pairs = _pairs([300, 517, 800, 1203, 64, 2600, 5200, 6100], seed0=400)
     for flags in (0, bm.BM_FLAG_FORCE_I32):
         with bm.Batch(pairs, flags) as B:
             B.set_mappings([g["map0"] for g in pairs])
